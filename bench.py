@@ -1,0 +1,365 @@
+"""Benchmark of the LES RK3 hot path (one JSON line on rank 0).
+
+Workload: the production channel grid nx=ny=512, nz=256 (67.1 M points,
+3/2-padded planes of 768x768), Re_tau=590, Deardorff TKE SGS, wall model
+isurface=6, seeded synthetic initial field (parabolic mean + uniform
+perturbations, projected divergence-free) built on the device, fixed dt at
+CFL 0.5.  A step is one full RK3 step (three stages of comp1 + comprhs +
+press + comp2) of the whole domain; metric = nx*ny*nz*steps / seconds.
+
+`value` is the plain FP64 drop-in form with the state resident in HBM;
+`forms` also reports the mixed form (FP32 transforms/advection/SGS, FP64
+pressure, mean modes and reductions).  `e2e` is the same metric through the
+C ABI a host program uses: the initial state is uploaded from pinned host
+memory inside the timed region and every step ends with les_gpu_stats
+(statistics read back to the host).
+
+--impl reference times the CPU restatement of the reference (oracle/, FP64,
+OpenMP on all host cores) on a 512x512x4 slab of the same grid (the cost
+per point depends on nx, ny, not nz), one RK3 step per timed step.
+
+Multi-GPU (torchrun): the domain is not decomposed (single-GPU tier, no MPI
+decomposition): each rank runs an independent replica; value = points*steps
+of all ranks / max-over-ranks time ("weak" scaling, replicas only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = 512
+NZ = 256
+RE_TAU = 590.0
+SLAB_NZ = 4
+METRIC = "RK3 Mpoint-steps/s"
+
+
+def load_product():
+    import importlib.util
+    name = "les_gpu_host"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "paes-channelflow_b200", "les_gpu.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(kernel, nx, ny, nz, tb):
+    """Compulsory HBM bytes of one launch (one stage over all levels) of the
+    stage kernels: every array the kernel must read once and write once."""
+    mx, my, kx = 3 * nx // 2, 3 * ny // 2, nx // 2
+    pad = mx * my * tb            # padded physical plane
+    mix = my * kx * 2 * tb        # x-spectral, y-physical plane on the padded y grid
+    spec = ny * kx * 2 * tb       # small spectrum plane
+    small = nx * ny * tb
+    L, Lw = nz, nz - 1            # levels of u, v | w, e
+    nm = ny * kx
+    table = {
+        "k_y_inverse": (2 * L + 2 * Lw) * spec + (4 * L + 4 * Lw) * mix,
+        "k_x_inverse": (4 * L + 4 * Lw) * mix + (6 * L + 6 * Lw) * pad,
+        "k_flux": (6 * L + 6 * Lw) * pad + (5 * L + 6 * Lw) * pad,
+        "k_x_forward": (5 * L + 6 * Lw) * pad + (4 * L + 4 * Lw) * mix,
+        "k_y_forward": (4 * L + 4 * Lw) * mix + (2 * L + Lw) * spec + Lw * spec,
+        "k_clip_y": Lw * pad * 2,
+        "k_clip_x": Lw * pad * 4,
+        "k_e_prep": Lw * (3 * small + spec),
+        "k_e_update": Lw * (spec + 3 * small),
+        "k_press": nz * (9 * spec + 2 * 24 * nm + 16 * nm),
+        "k_update": nz * (15 * spec + 16 * nm),
+    }
+    return table.get(kernel)
+
+
+def run_form(P, precision, steps, warmup, dev, want_profile):
+    import torch
+    cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=precision, device=dev)
+    g = P.LesGpu(cfg)
+    g.make_ic(seed=12345, amp=0.1, re_tau=RE_TAU)
+    dt = g.cfl_dt(0.5)
+    g.cfg.dt = dt
+    for i in range(warmup):
+        g.step(it=i + 1, mnout=False, dt=dt)
+    g.sync()
+    stream = torch.cuda.ExternalStream(g.stream_handle(), device=torch.device("cuda", dev))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = g.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        for i in range(steps):
+            g.step(it=warmup + i + 1, mnout=False, dt=dt)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = g.kernel_launches() - n0
+    g.sync()
+    out = {"ms": ms, "launches": launches, "clocks": clk.summary(), "dt": dt}
+    if want_profile:
+        prof = g.profile_stage(2, dt)
+        out["profile"] = prof
+    mb, sc = g.stats()
+    out["utau"] = float(sc[0])
+    out["divz_max"] = float(np.max(mb[2]))
+    out["handle"] = g
+    return out
+
+
+def run_e2e(P, steps, dev):
+    """Through the C ABI with host buffers: upload the state from pinned host
+    memory, then steps x (les_gpu_step + les_gpu_stats read-back)."""
+    import torch
+    cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=P.PREC_FP64, device=dev)
+    g = P.LesGpu(cfg)
+    g.make_ic(seed=12345, amp=0.1, re_tau=RE_TAU)
+    dt = g.cfl_dt(0.5)
+    shape = (NZ, NY, NX)
+    host = {k: torch.empty(shape, dtype=torch.float64, pin_memory=True) for k in "uvwep"}
+    g.download_into(*[host[k] for k in "uvwep"])
+    g.step(it=1, mnout=False, dt=dt)  # build the step graph outside the timed region
+    g.stats()
+    g.sync()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.upload(*[host[k] for k in "uvwep"])
+    for i in range(steps):
+        g.step(it=i + 2, mnout=False, dt=dt)
+        g.stats()
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    barrier()
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    d2h = (19 * NZ + 5) * 8
+    g.close()
+    return el, h2d / steps, d2h
+
+
+_pg = None
+
+
+def barrier():
+    if _pg is not None:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x):
+    if _pg is None:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(steps=1, threads=None):
+    """The oracle (CPU restatement of the reference, FP64) on a 512x512x4 slab."""
+    from oracle import oracle as O
+    lib = O.lib()
+    cfg = O.make_config(NX, NY, SLAB_NZ, dt=1e-3, re_tau=RE_TAU)
+    o = O.Oracle(cfg)
+    o.make_ic(seed=12345, amp=0.1, re_tau=RE_TAU)
+    o.set_dt(o.cfl_dt(0.5))
+    o.step(0, 1, 0)  # warm-up
+    t0 = time.perf_counter()
+    o.step(1, steps, 0)
+    el = time.perf_counter() - t0
+    pts = NX * NY * SLAB_NZ * steps
+    return pts / el / 1e6, lib.orc_threads(), el
+
+
+def main():
+    global _pg
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, local_rank, world = dist_env()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        per = []
+        for _ in range(args.warmup):
+            cpu_baseline(1)
+        for _ in range(args.steps):
+            v, cores, el = cpu_baseline(1)
+            per.append(el)
+        el = sum(per)
+        val = NX * NY * SLAB_NZ * args.steps / el / 1e6
+        line = {"metric": METRIC, "value": val, "unit": "Mpoint-steps/s", "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "channel 512x512x256 Re_tau=590 Deardorff isurface=6, sampled as a 512x512x4 slab",
+                           "global_batch": NX * NY * SLAB_NZ, "parallelism": "cpu-openmp"},
+                "cpu_baseline": {"value": val, "unit": "Mpoint-steps/s", "cores": cores, "kind": "port",
+                                 "sample": "512x512x4 slab of the 512x512x256 grid, 1 RK3 step per timed step, FP64 oracle"},
+                "e2e": {"value": val, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        _pg = dist.group.WORLD
+    dev = local_rank if world > 1 else 0
+    torch.cuda.set_device(dev)
+    P = load_product()
+
+    r64 = run_form(P, P.PREC_FP64, args.steps, args.warmup, dev, want_profile=True)
+    prof = r64.pop("profile")
+    r64.pop("handle").close()
+    r32 = run_form(P, P.PREC_MIXED, args.steps, args.warmup, dev, want_profile=False)
+    r32.pop("handle").close()
+    torch.cuda.empty_cache()
+    e2e_s, h2d, d2h = run_e2e(P, args.steps, dev)
+
+    pts = NX * NY * NZ
+    ms64 = max_over_ranks(r64["ms"])
+    ms32 = max_over_ranks(r32["ms"])
+    e2e_s = max_over_ranks(e2e_s)
+    value = world * pts * args.steps / (ms64 / 1e3) / 1e6
+    mixed = world * pts * args.steps / (ms32 / 1e3) / 1e6
+    e2e = world * pts * args.steps / e2e_s / 1e6
+
+    # roofline of the dominant kernel (per-kernel CUDA events on the handle's stream)
+    agg = {}
+    for name, t in prof:
+        base = name.split("<")[0]
+        agg.setdefault(base, [name, 0.0])
+        agg[base][1] += t
+    top = max(agg.items(), key=lambda kv: kv[1][1])
+    kname, (kfull, kms) = top[0], top[1]
+    peak, peak_kind = peaks()
+    ab = algorithmic_bytes(kname, NX, NY, NZ, 8)
+    achieved = ab / (kms / 1e3) / 1e9 if ab else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic_c5.txt")
+    if os.path.exists(tfile):
+        for ln in open(tfile):
+            f = ln.split()
+            if len(f) >= 3 and f[0] == kname:
+                traffic = float(f[2])
+    stage_ms = sum(t for _, t in prof)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpoint-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "channel 512x512x256 (3/2-padded 768x768), Re_tau=590, Deardorff TKE, isurface=6, "
+                               "RK3 at CFL 0.5, seeded projected random IC",
+                   "global_batch": pts * world, "seq_len": None, "parallelism": "replicas%d" % world,
+                   "l2": "working set (tens of GB) >> 126 MB L2; no flush needed"},
+        "forms": {"fp64": value, "mixed": mixed, "mixed_vs_fp64": mixed / value,
+                  "fp64_ms_per_step": ms64 / args.steps, "mixed_ms_per_step": ms32 / args.steps},
+        "e2e": {"value": e2e, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": r64["launches"],
+        "clocks": r64["clocks"],
+        "roofline": {"bound": "hbm", "kernel": kfull, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "kernel_ms": kms, "stage_ms": stage_ms,
+                     "algorithmic_bytes": ab},
+        "kernels_ms_stage2": {n: round(t, 4) for n, t in prof},
+        "physics": {"utau": r64["utau"], "divz_max": r64["divz_max"], "dt": r64["dt"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, el = cpu_baseline(1)
+        line["cpu_baseline"] = {"value": v, "unit": "Mpoint-steps/s", "cores": cores, "kind": "port",
+                                "sample": "512x512x4 slab of the 512x512x256 grid, 1 RK3 step, FP64 oracle, %.1f s" % el}
+    if rank == 0:
+        print(json.dumps(line))
+    if _pg is not None:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

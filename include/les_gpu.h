@@ -158,8 +158,23 @@ int les_gpu_make_ic(les_handle* h, unsigned long long seed, double ub,
  * state (les.F90:205-208). */
 int les_gpu_cfl_dt(les_handle* h, double cfl, double* dt);
 
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events after the library's. */
+void* les_gpu_stream(les_handle* h);
+
 /* Number of kernels launched through this handle so far. */
 long long les_gpu_kernel_launches(les_handle* h);
+
+/* Tracing: run one stage (not graph-captured) with a CUDA event recorded
+ * after every kernel on the handle's stream; ms[i] is the duration of the
+ * i-th kernel and kernels[i] its host stub address (match it against
+ * dladdr / the exported kernel symbols).  *nkernels receives the count; at
+ * most cap entries are written.  Advances the state by one stage. */
+int les_gpu_profile_stage(les_handle* h, int istage, double dt, double* ms,
+                          const void** kernels, int cap, int* nkernels);
+
+/* sizeof(les_config) as compiled into the library (binding sanity check). */
+size_t les_gpu_config_size(void);
 
 /* ---------------------------------------------------------------------
  * Operator-level entry points on caller-owned DEVICE buffers (FP64 or FP32
@@ -190,6 +205,9 @@ int les_op_deal(void* x, int nx, int ny, int howmany, int real_bytes,
  * overwrites bdar(:,:,4) and bdar(:,:,2) receives the inverted pivots, as
  * in the reference.  FP64 only (real_bytes = 8). */
 int les_op_tridv(void* bdar, int ny, int n, int real_bytes, void* stream);
+
+/* Message of the last failed les_op_* call on this thread. */
+const char* les_op_last_error(void);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,392 @@
+"""Host layer of the B200 LES hot path: ctypes bindings of libles_gpu.so
+(include/les_gpu.h) with the reference's per-stage interface.
+
+The reference drives one RK3 stage as (les.F90:254-285)::
+
+    lower; upper; comp1(it, mnout, istart, iend, nm, np, istage)
+    comprhs(istart, iend); press(...); comp2(istart, iend)
+
+`LesGpu` exposes the same calls on a device-resident domain (`lower`,
+`upper`, `comp1`, `comprhs`, `press`, `comp2`), the fused `stage` and
+graph-replayed `step`, and the lifecycle around them (init / upload /
+download / stats / spectra / finalize).  Every call goes through the C ABI;
+there is no CPU fallback: if the CUDA library or a device is missing, the
+constructor raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libles_gpu.so")
+
+LES_OK, LES_EINVAL, LES_ECUDA, LES_ENAN, LES_ETIMEOUT, LES_EUTAU, LES_ENOMEM, LES_ESTATE, LES_ENOTBUILT = range(9)
+SGS_DEARDORFF, SGS_SMAG, SGS_LEARNED = 3, 4, 5
+PREC_FP64, PREC_MIXED = 8, 4
+
+# RK3 coefficients of les.F90:26-27 (Wray's low-storage scheme)
+GAMA = (8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0)
+ZETAS = (0.0, 17.0 / 60.0, 5.0 / 12.0)
+
+
+class LesError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("les_gpu error %d: %s" % (code, msg))
+        self.code = code
+
+
+class LesConfig(ctypes.Structure):
+    """Mirror of `les_config` (include/les_gpu.h)."""
+
+    _fields_ = [
+        ("nnx", ctypes.c_int), ("nny", ctypes.c_int), ("nnz", ctypes.c_int),
+        ("imodel", ctypes.c_int), ("isurface", ctypes.c_int),
+        ("tke_production", ctypes.c_int), ("precision", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("xl", ctypes.c_double), ("yl", ctypes.c_double), ("zl", ctypes.c_double),
+        ("z0", ctypes.c_double), ("dt", ctypes.c_double),
+        ("cb", ctypes.c_double), ("skc", ctypes.c_double), ("nu", ctypes.c_double),
+        ("ugal", ctypes.c_double), ("vgal", ctypes.c_double), ("ufree", ctypes.c_double),
+        ("emin", ctypes.c_double), ("forcing", ctypes.c_double),
+    ]
+
+
+def channel_config(nnx, nny, nnz, dt=1e-3, re_tau=180.0, imodel=SGS_DEARDORFF, isurface=6,
+                   tke_production=0, precision=PREC_FP64, device=0, nu=0.0):
+    """Channel of the benchmark configurations: Lx=2pi, Ly=pi, walls at z=0
+    and z=2 (half height 1), forcing 0.016 (u_tau = sqrt(0.016)), and Re_tau
+    mapped onto the wall-model roughness z0 = exp(-kappa*B) h / Re_tau with
+    kappa=0.4, B=5 (the reference has no molecular viscosity)."""
+    c = LesConfig()
+    c.nnx, c.nny, c.nnz = nnx, nny, nnz
+    c.imodel, c.isurface, c.tke_production, c.precision, c.device = imodel, isurface, tke_production, precision, device
+    c.xl, c.yl, c.zl = 2 * np.pi, np.pi, 2.0
+    c.z0 = float(np.exp(-0.4 * 5.0) * 1.0 / re_tau)
+    c.dt = dt
+    c.cb, c.skc, c.nu = 0.0, 1.0, nu
+    c.ugal = c.vgal = c.ufree = 0.0
+    c.emin, c.forcing = 1e-6, 0.016
+    return c
+
+
+def bulk_velocity(re_tau, utau=float(np.sqrt(0.016)), kappa=0.4, b=5.0):
+    """Bulk mean of the log law over the half channel: ub/utau = (ln Re_tau - 1)/kappa + B."""
+    return utau * ((np.log(re_tau) - 1.0) / kappa + b)
+
+
+_lib = None
+
+
+def lib():
+    """Load libles_gpu.so (built in this directory); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise LesError(LES_ENOTBUILT, "libles_gpu.so not built: run `make -C %s`" % HERE)
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, D, VP = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    H = ctypes.c_void_p
+    sig = {
+        "les_gpu_default_config": (None, [ctypes.POINTER(LesConfig)]),
+        "les_gpu_config_size": (ctypes.c_size_t, []),
+        "les_gpu_init": (I, [ctypes.POINTER(LesConfig), ctypes.POINTER(H)]),
+        "les_gpu_finalize": (None, [H]),
+        "les_gpu_last_error": (ctypes.c_char_p, [H]),
+        "les_gpu_upload": (I, [H, VP, VP, VP, VP, VP, I]),
+        "les_gpu_download": (I, [H, VP, VP, VP, VP, VP, I]),
+        "les_gpu_upload_tendencies": (I, [H, VP, VP, VP, VP, I]),
+        "les_gpu_download_tendencies": (I, [H, VP, VP, VP, VP, I]),
+        "les_gpu_lower": (I, [H]),
+        "les_gpu_upper": (I, [H]),
+        "les_gpu_comp1": (I, [H, I, I, I, D, D, D]),
+        "les_gpu_comprhs": (I, [H, D]),
+        "les_gpu_press": (I, [H]),
+        "les_gpu_comp2": (I, [H, D]),
+        "les_gpu_stage": (I, [H, I, I, I, D, D, D]),
+        "les_gpu_step": (I, [H, I, I, D]),
+        "les_gpu_stats": (I, [H, VP, VP]),
+        "les_gpu_spectra": (I, [H, I, I, VP, VP]),
+        "les_gpu_sync": (I, [H, D]),
+        "les_gpu_make_ic": (I, [H, ctypes.c_ulonglong, D, D, D, D]),
+        "les_gpu_cfl_dt": (I, [H, D, ctypes.POINTER(D)]),
+        "les_gpu_kernel_launches": (ctypes.c_longlong, [H]),
+        "les_gpu_profile_stage": (I, [H, I, D, VP, VP, I, ctypes.POINTER(I)]),
+        "les_gpu_stream": (VP, [H]),
+        "les_op_xderiv": (I, [VP, VP, I, I, I, D, I, VP]),
+        "les_op_yderiv": (I, [VP, VP, I, I, I, D, I, VP]),
+        "les_op_expand": (I, [VP, VP, I, I, I, I, VP]),
+        "les_op_compress": (I, [VP, VP, I, I, I, I, VP]),
+        "les_op_deal": (I, [VP, I, I, I, I, VP]),
+        "les_op_tridv": (I, [VP, I, I, I, VP]),
+        "les_op_last_error": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    if L.les_gpu_config_size() != ctypes.sizeof(LesConfig):
+        raise LesError(LES_EINVAL, "les_config layout mismatch between header and bindings")
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Entry points declared in include/les_gpu.h."""
+    hdr = os.path.join(os.path.dirname(HERE), "include", "les_gpu.h")
+    import re
+    text = open(hdr).read()
+    return sorted(set(re.findall(r"\b(les_(?:gpu|op)_[a-z0-9_]+)\s*\(", text)))
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return int(a)
+
+
+class LesGpu:
+    """One device-resident channel domain (one handle, one CUDA stream).
+
+    Field arrays are (nnz, nny, nnx) C-ordered numpy arrays (== the
+    reference's column-major (nnx, nny, nnz) levels 1..nnz), float64 or
+    float32, or pinned torch tensors for asynchronous host transfers."""
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.shape = (cfg.nnz, cfg.nny, cfg.nnx)
+        h = ctypes.c_void_p()
+        rc = lib().les_gpu_init(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != LES_OK:
+            raise LesError(rc, lib().les_gpu_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().les_gpu_finalize(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != LES_OK:
+            raise LesError(rc, lib().les_gpu_last_error(self.h).decode())
+
+    @staticmethod
+    def _rb(arrs):
+        for a in arrs:
+            if a is None:
+                continue
+            if isinstance(a, np.ndarray):
+                return a.dtype.itemsize
+            return a.element_size()
+        return 8
+
+    # lifecycle / transfer
+    def upload(self, u=None, v=None, w=None, e=None, p=None):
+        arrs = [None if a is None else (np.ascontiguousarray(a) if isinstance(a, np.ndarray) else a)
+                for a in (u, v, w, e, p)]
+        self._check(lib().les_gpu_upload(self.h, *[_ptr(a) for a in arrs], self._rb(arrs)))
+
+    def download(self, dtype=np.float64, fields="uvwep"):
+        out = {k: np.zeros(self.shape, dtype=dtype) for k in fields}
+        self._check(lib().les_gpu_download(self.h, *[_ptr(out.get(k)) for k in "uvwep"], np.dtype(dtype).itemsize))
+        return out
+
+    def download_into(self, u=None, v=None, w=None, e=None, p=None):
+        arrs = (u, v, w, e, p)
+        self._check(lib().les_gpu_download(self.h, *[_ptr(a) for a in arrs], self._rb(arrs)))
+
+    def upload_tendencies(self, ru=None, rv=None, rw=None, re=None):
+        arrs = [None if a is None else np.ascontiguousarray(a) for a in (ru, rv, rw, re)]
+        self._check(lib().les_gpu_upload_tendencies(self.h, *[_ptr(a) for a in arrs], self._rb(arrs)))
+
+    def download_tendencies(self, dtype=np.float64):
+        out = {k: np.zeros(self.shape, dtype=dtype) for k in ("ru", "rv", "rw", "re")}
+        self._check(lib().les_gpu_download_tendencies(self.h, *[_ptr(out[k]) for k in ("ru", "rv", "rw", "re")],
+                                                      np.dtype(dtype).itemsize))
+        return out
+
+    # the reference's per-stage routines
+    def lower(self):
+        self._check(lib().les_gpu_lower(self.h))
+
+    def upper(self):
+        self._check(lib().les_gpu_upper(self.h))
+
+    def comp1(self, it, mnout, istage, dtab1, dtab2, xkmax):
+        self._check(lib().les_gpu_comp1(self.h, it, int(mnout), istage, dtab1, dtab2, xkmax))
+
+    def comprhs(self, dtabm):
+        self._check(lib().les_gpu_comprhs(self.h, dtabm))
+
+    def press(self):
+        self._check(lib().les_gpu_press(self.h))
+
+    def comp2(self, dtab1):
+        self._check(lib().les_gpu_comp2(self.h, dtab1))
+
+    def stage(self, it, mnout, istage, dt=None):
+        dt = self.cfg.dt if dt is None else dt
+        dz = self.cfg.zl / self.cfg.nnz
+        self._check(lib().les_gpu_stage(self.h, it, int(mnout), istage, dt * GAMA[istage - 1],
+                                        dt * ZETAS[istage - 1], dz * dz / dt / 5.0))
+
+    def stage_split(self, it, mnout, istage, dt=None):
+        """One stage through the six reference-named entry points."""
+        dt = self.cfg.dt if dt is None else dt
+        dz = self.cfg.zl / self.cfg.nnz
+        dtab1, dtab2 = dt * GAMA[istage - 1], dt * ZETAS[istage - 1]
+        self.lower()
+        self.upper()
+        self.comp1(it, mnout, istage, dtab1, dtab2, dz * dz / dt / 5.0)
+        self.comprhs(1.0 / dtab1)
+        self.press()
+        self.comp2(dtab1)
+
+    def step(self, it=1, mnout=False, dt=None):
+        dt = self.cfg.dt if dt is None else dt
+        self._check(lib().les_gpu_step(self.h, it, int(mnout), dt))
+
+    def sync(self, timeout_s=60.0):
+        self._check(lib().les_gpu_sync(self.h, timeout_s))
+
+    # diagnostics
+    def stats(self):
+        mb = np.zeros(19 * self.cfg.nnz)
+        sc = np.zeros(5)
+        self._check(lib().les_gpu_stats(self.h, _ptr(mb), _ptr(sc)))
+        return mb.reshape(self.cfg.nnz, 19).T.copy(), sc
+
+    def spectra(self, field, iz):
+        n = self.cfg.nnx // 2 + 1
+        a, b = np.zeros(n), np.zeros(n)
+        self._check(lib().les_gpu_spectra(self.h, field, iz, _ptr(a), _ptr(b)))
+        return a, b
+
+    def make_ic(self, seed=12345, ub=None, amp=0.1, utau=float(np.sqrt(0.016)), e0=1e-4, re_tau=180.0):
+        if ub is None:
+            ub = bulk_velocity(re_tau, utau)
+        self._check(lib().les_gpu_make_ic(self.h, seed, ub, amp, utau, e0))
+
+    def cfl_dt(self, cfl=0.5):
+        d = ctypes.c_double()
+        self._check(lib().les_gpu_cfl_dt(self.h, cfl, ctypes.byref(d)))
+        return d.value
+
+    def kernel_launches(self):
+        return lib().les_gpu_kernel_launches(self.h)
+
+    def stream_handle(self):
+        """The handle's cudaStream_t as an integer (torch.cuda.ExternalStream)."""
+        return lib().les_gpu_stream(self.h) or 0
+
+    def profile_stage(self, istage=2, dt=None):
+        """Run one stage eagerly with CUDA events between the kernels; returns
+        [(kernel name, ms)] in launch order (advances the state)."""
+        dt = self.cfg.dt if dt is None else dt
+        cap = 64
+        ms = (ctypes.c_double * cap)()
+        fn = (ctypes.c_void_p * cap)()
+        n = ctypes.c_int()
+        self._check(lib().les_gpu_profile_stage(self.h, istage, dt, ms, fn, cap, ctypes.byref(n)))
+        return [(kernel_name(fn[i]), ms[i]) for i in range(min(n.value, cap))]
+
+
+class _DlInfo(ctypes.Structure):
+    _fields_ = [("dli_fname", ctypes.c_char_p), ("dli_fbase", ctypes.c_void_p),
+                ("dli_sname", ctypes.c_char_p), ("dli_saddr", ctypes.c_void_p)]
+
+
+def kernel_name(addr):
+    """Short name of a kernel from its host stub address (dladdr + a light
+    demangling of les::k_<name><T, N>)."""
+    libdl = ctypes.CDLL(None)
+    info = _DlInfo()
+    if not addr or not libdl.dladdr(ctypes.c_void_p(addr), ctypes.byref(info)) or not info.dli_sname:
+        return hex(addr or 0)
+    raw = info.dli_sname.decode()
+    import re
+    m = re.match(r"_ZN3les(\d+)(k_\w+)", raw)
+    if not m:
+        return raw
+    n = int(m.group(1))
+    name = m.group(2)[:n]
+    tail = raw[m.end(1) + n:]
+    tp = "f64" if tail.startswith("IdL") or tail.startswith("Id") else ("f32" if tail.startswith("If") else "")
+    num = re.match(r"I[df]Li(\d+)", tail)
+    return name + ("<%s%s>" % (tp, "," + num.group(1) if num else "") if tp else "")
+
+
+# --- operator-level entry points on torch CUDA tensors (float64 or float32) ---
+def _op_check(rc):
+    if rc != LES_OK:
+        raise LesError(rc, lib().les_op_last_error().decode())
+
+
+def _stream(t):
+    import torch
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def xderiv(a, length, out=None):
+    """xderiv (filter_fftw.f90:138-187) of (howmany, n2, n1) planes."""
+    out = a.new_empty(a.shape) if out is None else out
+    n2, n1 = a.shape[-2], a.shape[-1]
+    howmany = a.numel() // (n1 * n2)
+    _op_check(lib().les_op_xderiv(a.data_ptr(), out.data_ptr(), n1, n2, howmany, length, a.element_size(), _stream(a)))
+    return out
+
+
+def yderiv(a, length, out=None):
+    """yderiv (filter_fftw.f90:194-248) of (howmany, n2, n1) planes."""
+    out = a.new_empty(a.shape) if out is None else out
+    n2, n1 = a.shape[-2], a.shape[-1]
+    howmany = a.numel() // (n1 * n2)
+    _op_check(lib().les_op_yderiv(a.data_ptr(), out.data_ptr(), n1, n2, howmany, length, a.element_size(), _stream(a)))
+    return out
+
+
+def expand(a):
+    """expand (filter_fftw.f90:254-278): (.., ny, nx) -> (.., 3ny/2, 3nx/2)."""
+    ny, nx = a.shape[-2], a.shape[-1]
+    howmany = a.numel() // (nx * ny)
+    out = a.new_empty(a.shape[:-2] + (3 * ny // 2, 3 * nx // 2))
+    _op_check(lib().les_op_expand(a.data_ptr(), out.data_ptr(), nx, ny, howmany, a.element_size(), _stream(a)))
+    return out
+
+
+def compress(a):
+    """compress (filter_fftw.f90:285-308): (.., 3ny/2, 3nx/2) -> (.., ny, nx)."""
+    nyb, nxb = a.shape[-2], a.shape[-1]
+    nx, ny = 2 * nxb // 3, 2 * nyb // 3
+    howmany = a.numel() // (nxb * nyb)
+    out = a.new_empty(a.shape[:-2] + (ny, nx))
+    _op_check(lib().les_op_compress(a.data_ptr(), out.data_ptr(), nx, ny, howmany, a.element_size(), _stream(a)))
+    return out
+
+
+def deal(a):
+    """deal (filter_fftw.f90:316-329), in place on a copy."""
+    out = a.clone()
+    ny, nx = a.shape[-2], a.shape[-1]
+    _op_check(lib().les_op_deal(out.data_ptr(), nx, ny, a.numel() // (nx * ny), a.element_size(), _stream(a)))
+    return out
+
+
+def tridv(bdar):
+    """tridv (tridv.f90:167-221) on a float64 CUDA tensor shaped (4, n, ny)."""
+    out = bdar.clone()
+    _, n, ny = out.shape
+    _op_check(lib().les_op_tridv(out.data_ptr(), ny, n, 8, _stream(out)))
+    return out
