@@ -206,6 +206,20 @@ int les_op_deal(void* x, int nx, int ny, int howmany, int real_bytes,
  * in the reference.  FP64 only (real_bytes = 8). */
 int les_op_tridv(void* bdar, int ny, int n, int real_bytes, void* stream);
 
+/* expand() without any device allocation.  It has no counterpart in the
+ * reference.  Same arguments and results as les_op_expand, which allocates
+ * its two scratch buffers per call; this variant keeps the scratch in a
+ * static 16 MiB device array instead, for callers that must not allocate
+ * device memory while they run (memory reserved up front by the host,
+ * allocation-free regions, allocator policies that ban hidden allocations).
+ * Limit: howmany*(nx/2)*(ny + 3*ny/2) complex values of scratch (16 bytes
+ * each for real_bytes = 8, 8 for 4) must fit in 16 MiB, else LES_EINVAL.
+ * Every device that loads the library keeps the array until exit; calls
+ * share it, so calls that overlap on the GPU race; the first call on each
+ * device does a one-time set-up and must come before any stream capture. */
+int les_op_expand_noalloc(const void* xsmall, void* xlarge, int nx, int ny,
+                          int howmany, int real_bytes, void* stream);
+
 /* Message of the last failed les_op_* call on this thread. */
 const char* les_op_last_error(void);
 

@@ -156,6 +156,10 @@ int check_config(const les_config* c, std::string& why) {
 
 // ---- operator level ----
 static thread_local std::string g_op_err;
+namespace les {
+// Message for les_op_last_error() from the other translation units.
+void set_op_error(const char* msg) { g_op_err = msg ? msg : ""; }
+}  // namespace les
 
 template <class F>
 static int op_guard(F&& fn) {
