@@ -145,6 +145,8 @@ def algorithmic_bytes(kernel, nx, ny, nz, tb):
         "k_e_update": Lw * (spec + 3 * small),
         "k_press": nz * (9 * spec + 2 * 24 * nm + 16 * nm),
         "k_update": nz * (15 * spec + 16 * nm),
+        # fused row kernel: reads the 8 mixed inputs, writes the 8 mixed outputs
+        "k_row_fused": 2 * (4 * L + 4 * Lw) * mix,
     }
     return table.get(kernel)
 

@@ -20,7 +20,7 @@
 #include <vector>
 
 #include "../../include/les_gpu.h"
-#include "les_kernels.cuh"
+#include "les_fused.cuh"
 
 namespace les {
 
@@ -163,8 +163,13 @@ struct Engine : EngineBase {
   // work
   DevBuf<cx<T>> Xe, rem;
   DevBuf<cx<T>> mixed[8];
-  DevBuf<T> pad[12];
-  DevBuf<T> flux[11];
+  DevBuf<T> pad[12];   // unfused path: padded physical fields
+  DevBuf<T> flux[11];  // unfused path: flux fields
+  // fused path (k_row_fused): clip corrections and wall-model planes
+  bool fused = false;
+  DevBuf<int> clipflag;
+  DevBuf<T> ephys, dEX, dEY, wallpl;
+  DevBuf<cx<T>> xout[8];  // Xu1..Xe2 written by k_row_fused (its inputs stay readable)
   DevBuf<double> divacc, sgsacc, wacc, acc;
   DevBuf<WallParams> wp;
   DevBuf<int> err;
@@ -200,8 +205,18 @@ struct Engine : EngineBase {
     e.alloc(ps * (NZ + 2)); re.alloc(ps * NZ);
     Xe.alloc(ns); rem.alloc(ns);
     for (auto& b : mixed) b.alloc(nmix * NZ);
-    for (auto& b : pad) b.alloc(pb * NZ);
-    for (auto& b : flux) b.alloc(pb * NZ);
+    // the fused row kernel covers the Deardorff model without the optional
+    // production term; Smagorinsky and tke_production use the unfused kernels
+    fused = (c.imodel == LES_SGS_DEARDORFF && c.tke_production == 0);
+    if (fused) {
+      clipflag.alloc(NZ);
+      ephys.alloc(pb * NZ); dEX.alloc(pb * NZ); dEY.alloc(pb * NZ);
+      wallpl.alloc(pb * 4);
+      for (auto& b : xout) b.alloc(nmix * NZ);
+    } else {
+      for (auto& b : pad) b.alloc(pb * NZ);
+      for (auto& b : flux) b.alloc(pb * NZ);
+    }
     divacc.alloc(NZ); sgsacc.alloc((size_t)NZ * 8); wacc.alloc((size_t)2 * kWallBlocks * 8); acc.alloc((size_t)NZ * 16);
     wp.alloc(1); err.alloc(1); amax.alloc(4);
     for (auto& b : phys) b.alloc(ps * (NZ + 2));
@@ -217,6 +232,8 @@ struct Engine : EngineBase {
     for (auto& b : mixed) b.release();
     for (auto& b : pad) b.release();
     for (auto& b : flux) b.release();
+    clipflag.release(); ephys.release(); dEX.release(); dEY.release(); wallpl.release();
+    for (auto& b : xout) b.release();
     for (auto& b : phys) b.release();
   }
   cudaStream_t stream() override { return st; }
@@ -405,6 +422,78 @@ struct Engine : EngineBase {
       launch(k_y_inverse<T, N>, dim3(cdiv(KX, CM::TC), NZ, 4), dim3(2 * CM::THREADS), 2 * CM::buf(), st, src, dst,
              KX, NZ, (T)ky0, tw);
     });
+    if (fused) {
+      fused_middle(a);
+    } else {
+      unfused_middle(a);
+    }
+    with_small(NY, [&](auto cn) {
+      constexpr int N = decltype(cn)::value;
+      using C = ColCfg<3 * N / 2, T>;
+      Ptr8 X{};
+      for (int i = 0; i < 8; i++) X.p[i] = fused ? xout[i].p : mixed[i].p;  // Xu1..Xe2
+      Ptr8 rn{};
+      rn.p[0] = run.p; rn.p[1] = rvn.p; rn.p[2] = rwn.p; rn.p[3] = rem.p;
+      size_t smem = 2 * C::buf() + (size_t)C::TC * N * sizeof(cx<T>);
+      launch(k_y_forward<T, N>, dim3(cdiv(KX, C::TC), NZ, 4), dim3(2 * C::THREADS), smem, st, X, rn, KX, NZ, (T)ky0,
+             (T)(1.0 / ((double)MX * MY)), tw);
+    });
+  }
+  // Wall-model plane sums from the physical U, V rows of levels 1 and nnz.
+  void wall_params_from(const T* U, const T* V, size_t upper_off, const StageArgs& a) {
+    (void)upper_off;
+    launch(k_wall_sums<T>, dim3(kWallBlocks, 2), dim3(256), 0, st, U, V, 2, pb, wacc.p);
+    launch(k_wall_final, dim3(1), dim3(32), 0, st, (const double*)wacc.p, (int)kWallBlocks, (const double*)mru.p,
+           (const double*)mrv.p, a, (double)pb, 0.4, zody, cfg.ufree, wp.p, err.p);
+  }
+  void fused_middle(const StageArgs& a) {
+    // clip flags and corrections of max(expand(e), emin)
+    LES_CUDA(cudaMemsetAsync(clipflag.p, 0, NZ * sizeof(int), st));
+    with_small(NX, [&](auto cn) {
+      constexpr int N = decltype(cn)::value;
+      using C = RowCfg<3 * N / 2>;
+      launch(k_clip_flag<T, N>, dim3(cdiv(MY / 2, C::NT), NZ - 1), dim3(C::THREADS), C::template smem<T>(), st,
+             (const cx<T>*)mixed[6].p, clipflag.p, MY, (T)cfg.emin, tw);
+      launch(k_clip_phys<T, N>, dim3(cdiv(MY / 2, C::NT), NZ - 1), dim3(C::THREADS), C::template smem<T>(), st,
+             (const cx<T>*)mixed[6].p, ephys.p, (const int*)clipflag.p, MY, tw);
+    });
+    with_small(NY, [&](auto cn) {
+      constexpr int N = decltype(cn)::value;
+      using C = ColCfg<3 * N / 2, T>;
+      launch(k_clipd_y<T, N>, dim3(cdiv(MX / 2, C::TC), NZ - 1), dim3(C::THREADS), C::buf(), st,
+             (const T*)ephys.p, dEY.p, (const int*)clipflag.p, MX, (T)cfg.emin, (T)ky0, tw);
+    });
+    with_small(NX, [&](auto cn) {
+      constexpr int N = decltype(cn)::value;
+      using C = RowCfg<3 * N / 2>;
+      launch(k_clipd_x<T, N>, dim3(cdiv(MY / 2, C::NT), NZ - 1), dim3(C::THREADS), C::template smem<T>(), st,
+             (const T*)ephys.p, dEX.p, (const int*)clipflag.p, MY, (T)cfg.emin, (T)kx0, tw);
+      // physical U, V at levels 1 and nnz for the wall model: wallpl = [U1, Unz, V1, Vnz]
+      using CR = RowCfg<3 * N / 2>;
+      const int lv[2] = {1, NZ};
+      for (int side = 0; side < 2; side++)
+        for (int fld = 0; fld < 2; fld++)
+          launch(k_row_c2r<T, 3 * N / 2>, dim3(cdiv(MY / 2 + 1, CR::NT)), dim3(CR::THREADS), CR::template smem<T>(),
+                 st, (const cx<T>*)(mixed[fld == 0 ? 0 : 2].p + (size_t)(lv[side] - 1) * nmix),
+                 wallpl.p + (size_t)(2 * fld + side) * pb, MY, KX, tw);
+    });
+    wall_params_from(wallpl.p, wallpl.p + 2 * pb, pb, a);
+    // the fused row kernel
+    FusedArgs fa{};
+    for (int i = 0; i < 8; i++) { fa.in.p[i] = mixed[i].p; fa.out.p[i] = xout[i].p; }
+    fa.dEX = dEX.p; fa.dEY = dEY.p; fa.clipflag = clipflag.p; fa.wp = wp.p;
+    fa.divacc = divacc.p; fa.sgsacc = sgsacc.p;
+    int nch = (int)cdiv(8 * 148, MY);
+    nch = std::max(1, std::min(nch, NZ / 8 > 0 ? NZ / 8 : 1));
+    fa.zchunk = (int)cdiv(NZ, nch);
+    nch = (int)cdiv(NZ, fa.zchunk);
+    with_small(NX, [&](auto cn) {
+      constexpr int N = decltype(cn)::value;
+      launch(k_row_fused<T, N>, dim3(MY, nch), dim3(FusedCfg<N>::THREADS), FusedCfg<N>::template smem<T>(), st, fa,
+             a, tw);
+    });
+  }
+  void unfused_middle(const StageArgs& a) {
     Ptr8 msrc{};
     for (int i = 0; i < 8; i++) msrc.p[i] = mixed[i].p;
     Ptr12 pd{};
@@ -446,15 +535,6 @@ struct Engine : EngineBase {
       using C = RowCfg<3 * N / 2>;
       launch(k_x_forward<T, N>, dim3(cdiv(MY, C::NT), NZ, 6), dim3(C::THREADS), C::template smem<T>(), st, fl, X, MY,
              NZ, (T)kx0, tw);
-    });
-    with_small(NY, [&](auto cn) {
-      constexpr int N = decltype(cn)::value;
-      using C = ColCfg<3 * N / 2, T>;
-      Ptr8 rn{};
-      rn.p[0] = run.p; rn.p[1] = rvn.p; rn.p[2] = rwn.p; rn.p[3] = rem.p;
-      size_t smem = 2 * C::buf() + (size_t)C::TC * N * sizeof(cx<T>);
-      launch(k_y_forward<T, N>, dim3(cdiv(KX, C::TC), NZ, 4), dim3(2 * C::THREADS), smem, st, X, rn, KX, NZ, (T)ky0,
-             (T)(1.0 / ((double)MX * MY)), tw);
     });
   }
   void e_update(double dtab1) {

@@ -1,0 +1,543 @@
+// les_fused.cuh -- the padded-grid part of comp1 as one kernel per (padded
+// y row, z chunk): inverse x transforms of the mixed arrays, the pointwise
+// advection / SGS fluxes, and the forward x transforms with -d/dx folded in,
+// without ever writing the padded physical fields to HBM.
+//
+// The CTA walks up its z chunk keeping a window of physical rows in shared
+// memory (levels z-1, z, z+1 of U, V, W, E, packed as complex rows U+iV and
+// W+iE), exactly the sliding window of comp1.f90:91-121 / 179-184 but along
+// one row of the padded plane.  Six warps each own one transform per phase:
+//   phase I   (inverse)  w0: U+iV (z+1)   w1: W+iE (z+1)   w2: UX+iVX (z)
+//                        w3: UY+iVY (z)   w4: WX+iWY (z)   w5: EX+iEY (le)
+//   phase II  (pointwise, all threads) the eleven flux rows of k_flux
+//   phase III (forward)  w0: A+iPu  w1: B+iPv  w2: C+iG  w3: D+iPw
+//                        w4: F+iPe  w5: H
+// Transforms are warp-synchronous four-step FFTs (lanes = N2 in pass A,
+// N1 in pass B, __syncwarp between passes); block barriers only separate
+// the three phases.
+#pragma once
+#include "les_kernels.cuh"
+
+namespace les {
+
+// Warp-level four-step transform of one length-N sequence in `buf`
+// (smem_fft_elems<N,false>(1) elements).  IN: load(n) from global memory or,
+// with IN_SMEM, buf in natural layout.  OUT: buf in natural layout.
+template <int N, int S, bool IN_SMEM, class T, class LoadF>
+__device__ __forceinline__ void warp_fft(cx<T>* buf, const cx<T>* __restrict__ tw, LoadF load) {
+  constexpr int N1 = Split<N>::N1;
+  constexpr int N2 = Split<N>::N2;
+  constexpr int LD = N2 + 1;
+  static_assert(N1 <= 32 && N2 <= 32, "warp transform needs N1, N2 <= 32");
+  const cx<T>* twn = tw + tw_off(N);
+  const int lane = threadIdx.x & 31;
+  {
+    cx<T> v[N1];
+    if (lane < N2) {
+#pragma unroll
+      for (int n1 = 0; n1 < N1; n1++) {
+        if constexpr (IN_SMEM) v[n1] = buf[lane + N2 * n1];
+        else v[n1] = load(lane + N2 * n1);
+      }
+    }
+    if (IN_SMEM) __syncwarp();
+    if (lane < N2) {
+      Dft<N1, S, T>::run(v);
+#pragma unroll
+      for (int k1 = 0; k1 < N1; k1++) {
+        cx<T> w = twn[lane * k1];
+        if (S > 0) w.y = -w.y;
+        buf[k1 * LD + lane] = (k1 == 0) ? v[k1] : cmul(v[k1], w);
+      }
+    }
+  }
+  __syncwarp();
+  {
+    cx<T> v[N2];
+    if (lane < N1) {
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) v[n2] = buf[lane * LD + n2];
+    }
+    __syncwarp();
+    if (lane < N1) {
+      Dft<N2, S, T>::run(v);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) buf[lane + N1 * k2] = v[k2];
+    }
+  }
+  __syncwarp();
+}
+
+// Three-pass warp Stockham transform (radices R1, R2, R3), in place in buf
+// (natural layout, N elements): each pass holds only N/32 values per lane,
+// which keeps FP64 register use below the two-pass form's N2-point DFT.
+template <int N, int R, int NS, int S, bool FIRST, class T, class LoadF>
+__device__ __forceinline__ void warp_stockham_pass(cx<T>* buf, const cx<T>* __restrict__ twn, LoadF load) {
+  constexpr int M = N / R;             // butterflies in this pass
+  constexpr int J = (M + 31) / 32;     // butterflies per lane
+  const int lane = threadIdx.x & 31;
+  cx<T> v[J][R];
+#pragma unroll
+  for (int jj = 0; jj < J; jj++) {
+    const int j = lane + 32 * jj;
+    if (j < M) {
+      const int k = j % NS;
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        cx<T> x;
+        if constexpr (FIRST) x = load(j + r * M);
+        else x = buf[j + r * M];
+        if (NS > 1 && r > 0) {
+          cx<T> w = twn[k * r * (N / (NS * R))];
+          if (S > 0) w.y = -w.y;
+          x = cmul(x, w);
+        }
+        v[jj][r] = x;
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int jj = 0; jj < J; jj++) {
+    const int j = lane + 32 * jj;
+    if (j < M) {
+      const int k = j % NS;
+      Dft<R, S, T>::run(v[jj]);
+      const int base = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; r++) buf[base + r * NS] = v[jj][r];
+    }
+  }
+  __syncwarp();
+}
+template <int N, int R1, int R2, int R3, int S, bool IN_SMEM, class T, class LoadF>
+__device__ __forceinline__ void warp_fft3(cx<T>* buf, const cx<T>* __restrict__ tw, LoadF load) {
+  static_assert(R1 * R2 * R3 == N, "radices must multiply to N");
+  const cx<T>* twn = tw + tw_off(N);
+  if constexpr (IN_SMEM) warp_stockham_pass<N, R1, 1, S, false, T>(buf, twn, load);
+  else warp_stockham_pass<N, R1, 1, S, true, T>(buf, twn, load);
+  warp_stockham_pass<N, R2, R1, S, false, T>(buf, twn, load);
+  warp_stockham_pass<N, R3, R1 * R2, S, false, T>(buf, twn, load);
+}
+// Which warp transform a (length, type) uses.
+template <int N, class T> struct WarpPlan { static constexpr bool three = false; };
+template <> struct WarpPlan<768, double> { static constexpr bool three = true; };
+template <int N, int S, bool IN_SMEM, class T, class LoadF>
+__device__ __forceinline__ void warp_transform(cx<T>* buf, const cx<T>* __restrict__ tw, LoadF load) {
+  if constexpr (WarpPlan<N, T>::three) warp_fft3<N, 8, 8, 12, S, IN_SMEM, T>(buf, tw, load);
+  else warp_fft<N, S, IN_SMEM, T>(buf, tw, load);
+}
+
+struct FusedArgs {
+  // mixed inputs (x-spectral, y physical on the padded grid): Um, UYm, Vm,
+  // VYm, Wm, WYm, Em, EYm; outputs Xu1, Xu2, Xv1, Xv2, Xw1, Xw2, Xe1, Xe2
+  Ptr8 in, out;
+  const void* dEX;       // clip corrections (padded physical, levels 1..nnz-1)
+  const void* dEY;
+  const int* clipflag;   // per level 1..nnz-1 (index z-1)
+  const WallParams* wp;
+  double* divacc;
+  double* sgsacc;
+  int zchunk;
+};
+
+template <int NSX> struct FusedCfg {
+  static constexpr int MX = 3 * NSX / 2;
+  static constexpr int BUF = smem_fft_elems<MX, false>(1);  // elements per transform buffer
+  static constexpr int NBUF = 13;  // 6 level slots (3 levels x 2), 6 work buffers, 1 carried tuw/tvw
+  static constexpr int THREADS = 192;
+  template <class T> static constexpr size_t smem() { return (size_t)NBUF * BUF * sizeof(cx<T>); }
+};
+
+template <class T, int NSX>
+__global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
+  constexpr int MX = 3 * NSX / 2;
+  constexpr int KX = NSX / 2;
+  constexpr int BUF = FusedCfg<NSX>::BUF;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+  cx<T>* work[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) work[i] = sm + (size_t)(6 + i) * BUF;
+  cx<T>* carry = sm + (size_t)12 * BUF;  // (TUW, TVW) of level z-1
+  // level slots: slot s holds (U+iV) at sm + (2s)*BUF and (W+iE) at sm + (2s+1)*BUF
+  auto UVs = [&](int s) { return sm + (size_t)(2 * s) * BUF; };
+  auto WEs = [&](int s) { return sm + (size_t)(2 * s + 1) * BUF; };
+
+  const int NZ = a.NZ, MY = a.MY;
+  const int y = blockIdx.x;
+  const int z0 = blockIdx.y * f.zchunk + 1;
+  const int z1 = min(z0 + f.zchunk - 1, NZ);
+  if (z0 > NZ) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const T kx0 = (T)a.kx0, dzm = (T)a.dzm, todzm = (T)a.todzm, emin = (T)a.emin;
+  const T xkmax = (T)a.xkmax, nu = (T)a.nu, c01 = (T)0.1 * (T)a.dsl;
+  const WallParams& wp = *f.wp;
+
+  auto mixrow = [&](int j, int z) -> const cx<T>* {
+    return reinterpret_cast<const cx<T>*>(f.in.p[j]) + ((size_t)(z - 1) * MY + y) * KX;
+  };
+  // complex row Z = A + iB of two real c2r outputs from x-spectral rows A, B
+  // (optional i*kx on each; NULL = zero row)
+  auto c2r_load = [&](const cx<T>* A, bool ma, const cx<T>* B, bool mb, int n) -> cx<T> {
+    int k = -1;
+    bool mir = false;
+    if (n < KX) k = n;
+    else if (n > MX - KX) { k = MX - n; mir = true; }
+    if (k < 0) return zero_cx<T>();
+    cx<T> av = A ? A[k] : zero_cx<T>(), bv = B ? B[k] : zero_cx<T>();
+    T kk = kx0 * (T)k;
+    if (ma) av = mul_i(av) * kk;
+    if (mb) bv = mul_i(bv) * kk;
+    if (k == 0) { av.y = 0; bv.y = 0; }
+    if (mir) { av = conj(av); bv = conj(bv); }
+    return mk(av.x - bv.y, av.y + bv.x);
+  };
+  // inverse transform of one (A, B) pair into buf
+  auto inv = [&](cx<T>* buf, const cx<T>* A, bool ma, const cx<T>* B, bool mb) {
+    warp_transform<MX, +1, false>(buf, tw, [&](int n) { return c2r_load(A, ma, B, mb, n); });
+  };
+  auto clipE = [&](cx<T>* we) {
+    for (int x = lane; x < MX; x += 32) we[x].y = tmax(we[x].y, emin);
+    __syncwarp();
+  };
+  auto xkk = [&](T e) { return tmin(c01 * sqrt(e), xkmax) + nu; };
+
+  // ---- prologue: slots for levels z0-1 and z0, carried tuw/tvw of z0-1 ----
+  int sm1 = 0, s0 = 1, sp1 = 2;  // slots of z-1, z, z+1
+  {
+    // one transform per warp, described by (destination, A, ikx on A, B, ikx on B, clip E)
+    cx<T>* dst = nullptr;
+    const cx<T>* A = nullptr;
+    const cx<T>* B = nullptr;
+    bool ma = false, mb = false, ce = false;
+    const int zm = z0 - 1;
+    if (z0 == 1) {
+      if (warp == 0) { dst = UVs(s0); A = mixrow(0, 1); B = mixrow(2, 1); }
+      if (warp == 1) { dst = WEs(s0); A = mixrow(4, 1); B = mixrow(6, 1); ce = true; }
+    } else {
+      if (warp == 0) { dst = UVs(sm1); A = mixrow(0, zm); B = mixrow(2, zm); }
+      if (warp == 1) { dst = WEs(sm1); A = mixrow(4, zm); B = mixrow(6, min(zm, NZ - 1)); ce = true; }
+      if (warp == 2) { dst = UVs(s0); A = mixrow(0, z0); B = mixrow(2, z0); }
+      if (warp == 3) { dst = WEs(s0); A = z0 < NZ ? mixrow(4, z0) : nullptr; B = mixrow(6, min(z0, NZ - 1)); ce = true; }
+      if (warp == 4) { dst = work[0]; A = mixrow(4, zm); ma = true; B = mixrow(5, zm); }  // WX + iWY at z0-1
+    }
+    if (dst) {
+      inv(dst, A, ma, B, mb);
+      if (ce) clipE(dst);
+    }
+  }
+  __syncthreads();
+  if (z0 == 1) {
+    for (int x = threadIdx.x; x < MX; x += blockDim.x) {
+      cx<T> uv = UVs(s0)[x];
+      UVs(sm1)[x] = zero_cx<T>();
+      WEs(sm1)[x] = mk((T)0, WEs(s0)[x].y);  // w(0) = 0, e(0) = e(1)
+      T tu, tv;
+      wall_stress<T>(wp.w[0], wp, a, 0, uv.x, uv.y, tu, tv);
+      carry[x] = mk(tu, tv);
+    }
+  } else {
+    for (int x = threadIdx.x; x < MX; x += blockDim.x) {
+      cx<T> uvm = UVs(sm1)[x], uv0 = UVs(s0)[x], wxy = work[0][x];
+      T xk = xkk(WEs(sm1)[x].y);
+      T uz = (uv0.x - uvm.x) * dzm, vz = (uv0.y - uvm.y) * dzm;
+      carry[x] = mk(-xk * (uz + wxy.x), -xk * (vz + wxy.y));
+    }
+  }
+  __syncthreads();
+
+  double divz_part = 0.0;
+  double sgs_part[6] = {0, 0, 0, 0, 0, 0};
+  for (int z = z0; z <= z1; z++) {
+    const int le = z < NZ - 2 ? z : NZ - 2;
+    // ---- phase I: inverse transforms (one per warp) ----
+    {
+      cx<T>* dst = nullptr;
+      const cx<T>* A = nullptr;
+      const cx<T>* B = nullptr;
+      bool ma = false, mb = false, ce = false, zero = false;
+      switch (warp) {
+        case 0:  // U + iV at z+1
+          dst = UVs(sp1);
+          if (z + 1 <= NZ) { A = mixrow(0, z + 1); B = mixrow(2, z + 1); } else zero = true;
+          break;
+        case 1:  // W + iE at z+1 (w = 0 above nnz-1, e clamped to level nnz-1)
+          dst = WEs(sp1);
+          A = (z + 1 <= NZ - 1) ? mixrow(4, z + 1) : nullptr;
+          B = mixrow(6, min(z + 1, NZ - 1));
+          ce = true;
+          break;
+        case 2: dst = work[0]; A = mixrow(0, z); B = mixrow(2, z); ma = mb = true; break;  // UX + iVX
+        case 3: dst = work[1]; A = mixrow(1, z); B = mixrow(3, z); break;                 // UY + iVY
+        case 4:                                                                           // WX + iWY
+          dst = work[2];
+          if (z <= NZ - 1) { A = mixrow(4, z); ma = true; B = mixrow(5, z); } else zero = true;
+          break;
+        default:  // EX + iEY at le
+          if (z <= NZ - 1) { dst = work[3]; A = mixrow(6, le); ma = true; B = mixrow(7, le); }
+          break;
+      }
+      if (zero) {
+        for (int x = lane; x < MX; x += 32) dst[x] = zero_cx<T>();
+        __syncwarp();
+      } else if (dst) {
+        inv(dst, A, ma, B, mb);
+        if (ce) clipE(dst);
+      }
+    }
+    __syncthreads();
+    // ---- phase II: fluxes (k_flux) ----
+    const bool top = (z == NZ);
+    const bool clip = (!top) && f.clipflag[le - 1];
+    const T* dEX = reinterpret_cast<const T*>(f.dEX) + ((size_t)(le - 1) * MY + y) * MX;
+    const T* dEY = reinterpret_cast<const T*>(f.dEY) + ((size_t)(le - 1) * MY + y) * MX;
+    for (int x = threadIdx.x; x < MX; x += blockDim.x) {
+      const cx<T> uvm = UVs(sm1)[x], uv0 = UVs(s0)[x], uv1 = UVs(sp1)[x];
+      const cx<T> wem = WEs(sm1)[x], we0 = WEs(s0)[x], we1 = WEs(sp1)[x];
+      const cx<T> dxv = work[0][x], dyv = work[1][x], wxy = work[2][x];
+      cx<T> exy = top ? zero_cx<T>() : work[3][x];
+      if (clip) { exy.x += dEX[x]; exy.y += dEY[x]; }
+      const cx<T> tprev = carry[x];
+      const T U0 = uv0.x, V0 = uv0.y, Um = uvm.x, Vm = uvm.y, U1 = uv1.x, V1 = uv1.y;
+      const T W0 = we0.x, Wm = wem.x, W1 = we1.x, E0 = we0.y, Em = wem.y, E1 = we1.y;
+      const T ux = dxv.x, vx = dxv.y, uy = dyv.x, vy = dyv.y;
+      const T xkm = xkk(Em), xk0 = xkk(E0);
+      const T s = xkm + xk0;
+      const T tuu = -s * ux, tvv = -s * vy, tuv = -s * (uy + vx) * (T)0.5;
+      T tuw0, tvw0;
+      if (top) {
+        wall_stress<T>(wp.w[1], wp, a, 1, U0, V0, tuw0, tvw0);
+      } else {
+        const T uz = (U1 - U0) * dzm, vz = (V1 - V0) * dzm;
+        tuw0 = -xk0 * (uz + wxy.x);
+        tvw0 = -xk0 * (vz + wxy.y);
+      }
+      const T wz0 = (W0 - Wm) * dzm;
+      const T tww0 = -(xkm + xk0) * wz0;
+      const T A = U0 * U0 + tuu, B = U0 * V0 + tuv, C = V0 * V0 + tvv;
+      const T Pu = -((U1 + U0) * W0 - (Um + U0) * Wm) * todzm + (T)a.forcing - (tuw0 - tprev.x) * dzm;
+      const T Pv = -((V1 + V0) * W0 - (Vm + V0) * Wm) * todzm - (tvw0 - tprev.y) * dzm;
+      work[0][x] = mk(A, Pu);
+      work[1][x] = mk(B, Pv);
+      if (!top) {
+        const T xkp = xkk(E1);
+        const T wz1 = (W1 - W0) * dzm;
+        const T tww1 = -(xk0 + xkp) * wz1;
+        const T D = (T)0.5 * (U0 + U1) * W0 + tuw0;
+        const T G = (T)0.5 * (V0 + V1) * W0 + tvw0;
+        const T hp = (T)0.5 * (W1 + W0), hm = (T)0.5 * (W0 + Wm);
+        const T Pw = -(hp * hp - hm * hm) * dzm - (tww1 - tww0) * dzm;
+        const T F = (T)0.5 * E0 * (U0 + U1) - (T)2 * xk0 * exy.x;
+        const T H = (T)0.5 * E0 * (V0 + V1) - (T)2 * xk0 * exy.y;
+        const T Pe = -(W1 * E1 - Wm * Em) * todzm +
+                     ((xkp + xk0) * (E1 - E0) - (xk0 + xkm) * (E0 - Em)) * (T)a.dzm2 - (T)a.ceps * E0 * sqrt(E0);
+        work[2][x] = mk(C, G);
+        work[3][x] = mk(D, Pw);
+        work[4][x] = mk(F, Pe);
+        work[5][x] = mk(H, (T)0);
+      } else {
+        work[2][x] = mk(C, (T)0);
+      }
+      carry[x] = mk(tuw0, tvw0);
+      const T d = ux + vy + wz0;
+      divz_part += (double)(d * d);
+      if (a.mnout_sgs) {
+        sgs_part[0] += (double)tuu; sgs_part[1] += (double)tvv; sgs_part[2] += (double)tuv;
+        sgs_part[3] += (double)tww0; sgs_part[4] += (double)tuw0; sgs_part[5] += (double)tvw0;
+      }
+    }
+    __syncthreads();
+    // per-level statistics of this row
+    {
+      double v1[1] = {divz_part};
+      block_sum_atomic<1>(v1, f.divacc + (z - 1));
+      divz_part = 0.0;
+      if (a.mnout_sgs) {
+        __syncthreads();
+        block_sum_atomic<6>(sgs_part, f.sgsacc + (size_t)(z - 1) * 8);
+#pragma unroll
+        for (int q = 0; q < 6; q++) sgs_part[q] = 0.0;
+      }
+    }
+    // ---- phase III: forward transforms, -d/dx, truncation to kx < nx/2 ----
+    if (!(top && warp >= 3)) {
+      cx<T>* buf = work[warp];
+      warp_transform<MX, -1, true>(buf, tw, NoLoad{});
+      const size_t orow = ((size_t)(z - 1) * MY + y) * KX;
+      auto O = [&](int j) { return reinterpret_cast<cx<T>*>(f.out.p[j]) + orow; };
+      for (int k = lane; k < KX; k += 32) {
+        cx<T> zk = buf[k], zmr = conj(buf[(MX - k) % MX]);
+        cx<T> ah = (zk + zmr) * (T)0.5;
+        cx<T> dd = zk - zmr;
+        cx<T> bh = mk(dd.y * (T)0.5, -dd.x * (T)0.5);
+        T kk = kx0 * (T)k;
+        cx<T> dxa = mk(kk * ah.y, -kk * ah.x);  // -i kx a^
+        switch (warp) {
+          case 0: O(0)[k] = dxa + bh; break;                          // Xu1
+          case 1: O(2)[k] = dxa + bh; O(1)[k] = ah; break;            // Xv1, Xu2
+          case 2: O(3)[k] = ah; if (!top) O(5)[k] = bh; break;        // Xv2, Xw2
+          case 3: O(4)[k] = dxa + bh; break;                          // Xw1
+          case 4: O(6)[k] = dxa + bh; break;                          // Xe1
+          default: O(7)[k] = ah; break;                               // Xe2
+        }
+      }
+    }
+    __syncthreads();
+    // rotate the window: z -> z-1, z+1 -> z
+    const int t = sm1;
+    sm1 = s0; s0 = sp1; sp1 = t;
+  }
+}
+
+// Per-level flag: does max(expand(e), emin) clip anywhere on the padded
+// plane?  Rows of Em (pairs) are inverted and compared with emin.
+template <class T, int NSX>
+__global__ void __launch_bounds__(RowCfg<3 * NSX / 2>::THREADS)
+k_clip_flag(const cx<T>* __restrict__ Em, int* __restrict__ flags, int MY, T emin, const cx<T>* __restrict__ tw) {
+  constexpr int MX = 3 * NSX / 2;
+  constexpr int KX = NSX / 2;
+  using C = RowCfg<MX>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  const int z = blockIdx.y + 1;
+  const int p0 = blockIdx.x * C::NT, np = MY / 2;
+  const cx<T>* in = Em + (size_t)(z - 1) * MY * KX;
+  fft_core<MX, +1, false, false, false>(C::NT, sm, tw, [&](int t, int n) {
+    int p = p0 + t;
+    cx<T> v = zero_cx<T>();
+    if (p < np) {
+      int k = -1;
+      bool mir = false;
+      if (n < KX) k = n;
+      else if (n > MX - KX) { k = MX - n; mir = true; }
+      if (k >= 0) {
+        cx<T> av = in[(size_t)(2 * p) * KX + k], bv = in[(size_t)(2 * p + 1) * KX + k];
+        if (k == 0) { av.y = 0; bv.y = 0; }
+        if (mir) { av = conj(av); bv = conj(bv); }
+        v = mk(av.x - bv.y, av.y + bv.x);
+      }
+    }
+    return v;
+  }, [&](int t, int n, cx<T> v) {
+    int p = p0 + t;
+    if (p < np && (v.x < emin || v.y < emin)) any = 1;
+  });
+  __syncthreads();
+  if (threadIdx.x == 0 && any) atomicOr(flags + (z - 1), 1);
+}
+
+// Physical E (unclipped) of flagged levels, for the clip corrections.
+template <class T, int NSX>
+__global__ void __launch_bounds__(RowCfg<3 * NSX / 2>::THREADS)
+k_clip_phys(const cx<T>* __restrict__ Em, T* __restrict__ E, const int* __restrict__ flags, int MY,
+            const cx<T>* __restrict__ tw) {
+  constexpr int MX = 3 * NSX / 2;
+  constexpr int KX = NSX / 2;
+  using C = RowCfg<MX>;
+  const int z = blockIdx.y + 1;
+  if (!flags[z - 1]) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+  const int p0 = blockIdx.x * C::NT, np = MY / 2;
+  const cx<T>* in = Em + (size_t)(z - 1) * MY * KX;
+  T* out = E + (size_t)(z - 1) * MY * MX;
+  fft_core<MX, +1, false, false, false>(C::NT, sm, tw, [&](int t, int n) {
+    int p = p0 + t;
+    cx<T> v = zero_cx<T>();
+    if (p < np) {
+      int k = -1;
+      bool mir = false;
+      if (n < KX) k = n;
+      else if (n > MX - KX) { k = MX - n; mir = true; }
+      if (k >= 0) {
+        cx<T> av = in[(size_t)(2 * p) * KX + k], bv = in[(size_t)(2 * p + 1) * KX + k];
+        if (k == 0) { av.y = 0; bv.y = 0; }
+        if (mir) { av = conj(av); bv = conj(bv); }
+        v = mk(av.x - bv.y, av.y + bv.x);
+      }
+    }
+    return v;
+  }, [&](int t, int n, cx<T> v) {
+    int p = p0 + t;
+    if (p >= np) return;
+    out[(size_t)(2 * p) * MX + n] = v.x;
+    out[(size_t)(2 * p + 1) * MX + n] = v.y;
+  });
+}
+
+// dEY = yderiv(delta), delta = max(emin - E, 0), flagged levels only.
+template <class T, int NSY>
+__global__ void __launch_bounds__(ColCfg<3 * NSY / 2, T>::THREADS)
+k_clipd_y(const T* __restrict__ E, T* __restrict__ dEY, const int* __restrict__ flags, int MX, T emin, T ky0,
+          const cx<T>* __restrict__ tw) {
+  constexpr int M = 3 * NSY / 2;
+  using C = ColCfg<M, T>;
+  if (!flags[blockIdx.y]) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+  const size_t zoff = (size_t)blockIdx.y * M * MX;
+  const int c0 = blockIdx.x * C::TC, ncp = MX / 2;
+  const cx<T>* Ez = reinterpret_cast<const cx<T>*>(E + zoff);
+  fft_core<M, -1, true, false, true>(C::TC, sm, tw, [&](int t, int n) {
+    int c = c0 + t;
+    cx<T> v = zero_cx<T>();
+    if (c < ncp) {
+      cx<T> ev = Ez[(size_t)n * ncp + c];
+      v = mk(tmax(emin - ev.x, (T)0), tmax(emin - ev.y, (T)0));
+    }
+    return v;
+  }, NoStore{});
+  for (int i = threadIdx.x; i < C::TC * M; i += blockDim.x) {
+    int t = i % C::TC, k = i / C::TC;
+    T kk = (k == 0 || 2 * k == M) ? (T)0 : ky0 * (T)signed_k(k, M) / (T)M;
+    sm[k * C::TC + t] = mul_i(sm[k * C::TC + t]) * kk;
+  }
+  __syncthreads();
+  cx<T>* out = reinterpret_cast<cx<T>*>(dEY + zoff);
+  fft_core<M, +1, true, true, false>(C::TC, sm, tw, NoLoad{}, [&](int t, int n, cx<T> d) {
+    int c = c0 + t;
+    if (c < ncp) out[(size_t)n * ncp + c] = d;
+  });
+}
+
+// dEX = xderiv(delta), flagged levels only.
+template <class T, int NSX>
+__global__ void __launch_bounds__(RowCfg<3 * NSX / 2>::THREADS)
+k_clipd_x(const T* __restrict__ E, T* __restrict__ dEX, const int* __restrict__ flags, int MY, T emin, T kx0,
+          const cx<T>* __restrict__ tw) {
+  constexpr int MX = 3 * NSX / 2;
+  using C = RowCfg<MX>;
+  if (!flags[blockIdx.y]) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+  const size_t zoff = (size_t)blockIdx.y * MY * MX;
+  const int p0 = blockIdx.x * C::NT, np = MY / 2;
+  const T* Ez = E + zoff;
+  T* out = dEX + zoff;
+  fft_core<MX, -1, false, false, true>(C::NT, sm, tw, [&](int t, int n) {
+    int p = p0 + t;
+    cx<T> v = zero_cx<T>();
+    if (p < np) {
+      T av = Ez[(size_t)(2 * p) * MX + n], bv = Ez[(size_t)(2 * p + 1) * MX + n];
+      v = mk(tmax(emin - av, (T)0), tmax(emin - bv, (T)0));
+    }
+    return v;
+  }, NoStore{});
+  for (int i = threadIdx.x; i < C::NT * MX; i += blockDim.x) {
+    int t = i / MX, k = i - t * MX;
+    T kk = (k == 0 || 2 * k == MX) ? (T)0 : kx0 * (T)signed_k(k, MX) / (T)MX;
+    sm[t * MX + k] = mul_i(sm[t * MX + k]) * kk;
+  }
+  __syncthreads();
+  fft_core<MX, +1, false, true, false>(C::NT, sm, tw, NoLoad{}, [&](int t, int n, cx<T> d) {
+    int p = p0 + t;
+    if (p >= np) return;
+    out[(size_t)(2 * p) * MX + n] = d.x;
+    out[(size_t)(2 * p + 1) * MX + n] = d.y;
+  });
+}
+
+}  // namespace les
