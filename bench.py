@@ -299,7 +299,8 @@ def main():
     r64 = run_form(P, P.PREC_FP64, args.steps, args.warmup, dev, want_profile=True)
     prof = r64.pop("profile")
     r64.pop("handle").close()
-    r32 = run_form(P, P.PREC_MIXED, args.steps, args.warmup, dev, want_profile=False)
+    r32 = run_form(P, P.PREC_MIXED, args.steps, args.warmup, dev, want_profile=True)
+    prof32 = r32.pop("profile")
     r32.pop("handle").close()
     torch.cuda.empty_cache()
     e2e_s, h2d, d2h = run_e2e(P, args.steps, dev)
@@ -350,6 +351,7 @@ def main():
                      "peak_source": peak_kind, "kernel_ms": kms, "stage_ms": stage_ms,
                      "algorithmic_bytes": ab},
         "kernels_ms_stage2": {n: round(t, 4) for n, t in prof},
+        "kernels_ms_stage2_mixed": {n: round(t, 4) for n, t in prof32},
         "physics": {"utau": r64["utau"], "divz_max": r64["divz_max"], "dt": r64["dt"]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

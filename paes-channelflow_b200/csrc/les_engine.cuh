@@ -537,13 +537,18 @@ struct Engine : EngineBase {
              NZ, (T)kx0, tw);
     });
   }
+  // comp2's e update: re = c2r(rem) with plain stores, then the clipped
+  // elementwise update (a read-modify-write inside the transform's store
+  // phase would serialise on the load latency)
   void e_update(double dtab1) {
     with_small(NX, [&](auto cn) {
       constexpr int N = decltype(cn)::value;
       using C = RowCfg<N>;
-      launch(k_e_update<T, N>, dim3(cdiv(NY / 2, C::NT), NZ - 1), dim3(C::THREADS), C::template smem<T>(), st,
-             (const cx<T>*)rem.p, re.p, e.p, NY, (T)dtab1, (T)cfg.emin, tw);
+      launch(k_row_c2r<T, N>, dim3(cdiv((size_t)(NZ - 1) * NY / 2 + 1, C::NT)), dim3(C::THREADS),
+             C::template smem<T>(), st, (const cx<T>*)rem.p, re.p, (NZ - 1) * NY, KX, tw);
     });
+    launch(k_e_update_phys<T>, dim3(cdiv(ps * (NZ - 1), 256)), dim3(256), 0, st, e.p + ps, (const T*)re.p,
+           ps * (NZ - 1), (T)dtab1, (T)cfg.emin);
   }
   void press_kernel(const StageArgs& a, bool rhs_in_ph) {
     if (rhs_in_ph)

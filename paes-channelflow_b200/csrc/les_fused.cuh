@@ -20,23 +20,32 @@
 
 namespace les {
 
+// XOR swizzle of natural-layout indices in the fused kernel's buffers:
+// within each 128-byte block the low bits are XORed with the block index, so
+// strided butterfly writes (stride R elements) land in distinct banks.  A
+// bijection on [0, N) when N is a multiple of the block length.
+template <class T, int N> struct Swz {
+  static constexpr int SHIFT = (sizeof(cx<T>) == 16) ? 3 : 4;
+  static constexpr int MASK = (N % (1 << SHIFT) == 0) ? ((1 << SHIFT) - 1) : 0;
+  static __device__ __forceinline__ int f(int a) { return a ^ ((a >> SHIFT) & MASK); }
+};
+
 // Warp-level four-step transform of one length-N sequence in `buf`
 // (smem_fft_elems<N,false>(1) elements).  IN: load(n) from global memory or,
 // with IN_SMEM, buf in natural layout.  OUT: buf in natural layout.
 template <int N, int S, bool IN_SMEM, class T, class LoadF>
-__device__ __forceinline__ void warp_fft(cx<T>* buf, const cx<T>* __restrict__ tw, LoadF load) {
+__device__ __forceinline__ void warp_fft(cx<T>* buf, const cx<T>* twn, LoadF load) {
   constexpr int N1 = Split<N>::N1;
   constexpr int N2 = Split<N>::N2;
   constexpr int LD = N2 + 1;
   static_assert(N1 <= 32 && N2 <= 32, "warp transform needs N1, N2 <= 32");
-  const cx<T>* twn = tw + tw_off(N);
   const int lane = threadIdx.x & 31;
   {
     cx<T> v[N1];
     if (lane < N2) {
 #pragma unroll
       for (int n1 = 0; n1 < N1; n1++) {
-        if constexpr (IN_SMEM) v[n1] = buf[lane + N2 * n1];
+        if constexpr (IN_SMEM) v[n1] = buf[Swz<T, N>::f(lane + N2 * n1)];
         else v[n1] = load(lane + N2 * n1);
       }
     }
@@ -62,31 +71,37 @@ __device__ __forceinline__ void warp_fft(cx<T>* buf, const cx<T>* __restrict__ t
     if (lane < N1) {
       Dft<N2, S, T>::run(v);
 #pragma unroll
-      for (int k2 = 0; k2 < N2; k2++) buf[lane + N1 * k2] = v[k2];
+      for (int k2 = 0; k2 < N2; k2++) buf[Swz<T, N>::f(lane + N1 * k2)] = v[k2];
     }
   }
   __syncwarp();
 }
 
-// Three-pass warp Stockham transform (radices R1, R2, R3), in place in buf
-// (natural layout, N elements): each pass holds only N/32 values per lane,
-// which keeps FP64 register use below the two-pass form's N2-point DFT.
-template <int N, int R, int NS, int S, bool FIRST, class T, class LoadF>
-__device__ __forceinline__ void warp_stockham_pass(cx<T>* buf, const cx<T>* __restrict__ twn, LoadF load) {
-  constexpr int M = N / R;             // butterflies in this pass
-  constexpr int J = (M + 31) / 32;     // butterflies per lane
-  const int lane = threadIdx.x & 31;
+// Team Stockham transform: TEAM threads (a multiple of 32) share one
+// transform and synchronise with a named barrier `bar` (1..15), so several
+// teams run independent transforms inside one CTA.  In place in buf
+// (natural layout, N elements); each pass holds ceil(N/R/TEAM)*R values
+// per thread.
+template <int TEAM>
+__device__ __forceinline__ void team_sync(int bar) {
+  if (TEAM == 32) __syncwarp();
+  else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(TEAM) : "memory");
+}
+template <int N, int R, int NS, int S, bool FIRST, int TEAM, class T, class LoadF>
+__device__ __forceinline__ void team_stockham_pass(cx<T>* buf, const cx<T>* twn, LoadF load, int tl, int bar) {
+  constexpr int M = N / R;
+  constexpr int J = (M + TEAM - 1) / TEAM;
   cx<T> v[J][R];
 #pragma unroll
   for (int jj = 0; jj < J; jj++) {
-    const int j = lane + 32 * jj;
+    const int j = tl + TEAM * jj;
     if (j < M) {
       const int k = j % NS;
 #pragma unroll
       for (int r = 0; r < R; r++) {
         cx<T> x;
         if constexpr (FIRST) x = load(j + r * M);
-        else x = buf[j + r * M];
+        else x = buf[Swz<T, N>::f(j + r * M)];
         if (NS > 1 && r > 0) {
           cx<T> w = twn[k * r * (N / (NS * R))];
           if (S > 0) w.y = -w.y;
@@ -96,36 +111,50 @@ __device__ __forceinline__ void warp_stockham_pass(cx<T>* buf, const cx<T>* __re
       }
     }
   }
-  __syncwarp();
+  team_sync<TEAM>(bar);
 #pragma unroll
   for (int jj = 0; jj < J; jj++) {
-    const int j = lane + 32 * jj;
+    const int j = tl + TEAM * jj;
     if (j < M) {
       const int k = j % NS;
       Dft<R, S, T>::run(v[jj]);
       const int base = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; r++) buf[base + r * NS] = v[jj][r];
+      for (int r = 0; r < R; r++) buf[Swz<T, N>::f(base + r * NS)] = v[jj][r];
     }
   }
-  __syncwarp();
+  team_sync<TEAM>(bar);
 }
-template <int N, int R1, int R2, int R3, int S, bool IN_SMEM, class T, class LoadF>
-__device__ __forceinline__ void warp_fft3(cx<T>* buf, const cx<T>* __restrict__ tw, LoadF load) {
+template <int N> struct Radix3;
+template <> struct Radix3<24> { static constexpr int R1 = 2, R2 = 2, R3 = 6; };
+template <> struct Radix3<48> { static constexpr int R1 = 4, R2 = 2, R3 = 6; };
+template <> struct Radix3<96> { static constexpr int R1 = 4, R2 = 4, R3 = 6; };
+template <> struct Radix3<144> { static constexpr int R1 = 4, R2 = 6, R3 = 6; };
+template <> struct Radix3<192> { static constexpr int R1 = 8, R2 = 4, R3 = 6; };
+template <> struct Radix3<288> { static constexpr int R1 = 8, R2 = 6, R3 = 6; };
+template <> struct Radix3<384> { static constexpr int R1 = 8, R2 = 8, R3 = 6; };
+template <> struct Radix3<576> { static constexpr int R1 = 8, R2 = 6, R3 = 12; };
+template <> struct Radix3<768> { static constexpr int R1 = 8, R2 = 8, R3 = 12; };
+template <int N, int S, bool IN_SMEM, int TEAM, class T, class LoadF>
+__device__ __forceinline__ void team_fft(cx<T>* buf, const cx<T>* twn, LoadF load, int tl, int bar) {
+  constexpr int R1 = Radix3<N>::R1, R2 = Radix3<N>::R2, R3 = Radix3<N>::R3;
   static_assert(R1 * R2 * R3 == N, "radices must multiply to N");
-  const cx<T>* twn = tw + tw_off(N);
-  if constexpr (IN_SMEM) warp_stockham_pass<N, R1, 1, S, false, T>(buf, twn, load);
-  else warp_stockham_pass<N, R1, 1, S, true, T>(buf, twn, load);
-  warp_stockham_pass<N, R2, R1, S, false, T>(buf, twn, load);
-  warp_stockham_pass<N, R3, R1 * R2, S, false, T>(buf, twn, load);
+  team_stockham_pass<N, R1, 1, S, !IN_SMEM, TEAM, T>(buf, twn, load, tl, bar);
+  team_stockham_pass<N, R2, R1, S, false, TEAM, T>(buf, twn, load, tl, bar);
+  team_stockham_pass<N, R3, R1 * R2, S, false, TEAM, T>(buf, twn, load, tl, bar);
 }
-// Which warp transform a (length, type) uses.
-template <int N, class T> struct WarpPlan { static constexpr bool three = false; };
-template <> struct WarpPlan<768, double> { static constexpr bool three = true; };
+
+// Transform used by the fused kernel for a (length, type): the two-pass
+// warp form unless its N2-point register DFT would not fit (FP64 at 768),
+// then the three-pass Stockham form.
+template <int N, class T> struct FusedPlan {
+  static constexpr bool three = (sizeof(T) == 8 && Split<N>::N2 > 24);
+  static constexpr int BUF = three ? N : smem_fft_elems<N, false>(1);
+};
 template <int N, int S, bool IN_SMEM, class T, class LoadF>
-__device__ __forceinline__ void warp_transform(cx<T>* buf, const cx<T>* __restrict__ tw, LoadF load) {
-  if constexpr (WarpPlan<N, T>::three) warp_fft3<N, 8, 8, 12, S, IN_SMEM, T>(buf, tw, load);
-  else warp_fft<N, S, IN_SMEM, T>(buf, tw, load);
+__device__ __forceinline__ void fused_fft(cx<T>* buf, const cx<T>* twn, LoadF load, int lane) {
+  if constexpr (FusedPlan<N, T>::three) team_fft<N, S, IN_SMEM, 32, T>(buf, twn, load, lane, 0);
+  else warp_fft<N, S, IN_SMEM, T>(buf, twn, load);
 }
 
 struct FusedArgs {
@@ -143,23 +172,34 @@ struct FusedArgs {
 
 template <int NSX> struct FusedCfg {
   static constexpr int MX = 3 * NSX / 2;
-  static constexpr int BUF = smem_fft_elems<MX, false>(1);  // elements per transform buffer
-  static constexpr int NBUF = 13;  // 6 level slots (3 levels x 2), 6 work buffers, 1 carried tuw/tvw
-  static constexpr int THREADS = 192;
-  template <class T> static constexpr size_t smem() { return (size_t)NBUF * BUF * sizeof(cx<T>); }
+  static constexpr int NBUF = 11;  // 6 level slots (3 levels x 2), 4 work buffers, 1 carried tuw/tvw
+  static constexpr int TEAM = 32;  // one warp per transform
+  static constexpr int THREADS = 6 * TEAM;
+  template <class T> static constexpr int buf() { return FusedPlan<MX, T>::BUF; }
+  // buffers + the twiddle table of length MX staged in shared memory
+  template <class T> static constexpr size_t smem() {
+    return ((size_t)NBUF * buf<T>() + MX) * sizeof(cx<T>);
+  }
 };
 
 template <class T, int NSX>
-__global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(192, (sizeof(T) == 4) ? 2 : 1)
+k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   constexpr int MX = 3 * NSX / 2;
   constexpr int KX = NSX / 2;
-  constexpr int BUF = FusedCfg<NSX>::BUF;
+  constexpr int BUF = FusedCfg<NSX>::template buf<T>();
+  constexpr int TEAM = FusedCfg<NSX>::TEAM;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+  // twiddles exp(-2 pi i j / MX) staged once per CTA: every transform pass
+  // reads them from shared memory instead of the global table
+  cx<T>* tws = sm + (size_t)11 * BUF;
+  for (int j = threadIdx.x; j < MX; j += blockDim.x) tws[j] = tw[tw_off(MX) + j];
+  __syncthreads();
   cx<T>* work[6];
 #pragma unroll
-  for (int i = 0; i < 6; i++) work[i] = sm + (size_t)(6 + i) * BUF;
-  cx<T>* carry = sm + (size_t)12 * BUF;  // (TUW, TVW) of level z-1
+  for (int i = 0; i < 4; i++) work[i] = sm + (size_t)(6 + i) * BUF;
+  cx<T>* carry = sm + (size_t)10 * BUF;  // (TUW, TVW) of level z-1
   // level slots: slot s holds (U+iV) at sm + (2s)*BUF and (W+iE) at sm + (2s+1)*BUF
   auto UVs = [&](int s) { return sm + (size_t)(2 * s) * BUF; };
   auto WEs = [&](int s) { return sm + (size_t)(2 * s + 1) * BUF; };
@@ -169,7 +209,10 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
   const int z0 = blockIdx.y * f.zchunk + 1;
   const int z1 = min(z0 + f.zchunk - 1, NZ);
   if (z0 > NZ) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // team w (threads [64w, 64w+64)) owns transform w of every phase
+  const int warp = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
+  const int bar = 1 + warp;
+  auto S = [](int q) { return Swz<T, MX>::f(q); };  // swizzled position of element q
   const T kx0 = (T)a.kx0, dzm = (T)a.dzm, todzm = (T)a.todzm, emin = (T)a.emin;
   const T xkmax = (T)a.xkmax, nu = (T)a.nu, c01 = (T)0.1 * (T)a.dsl;
   const WallParams& wp = *f.wp;
@@ -193,13 +236,13 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
     if (mir) { av = conj(av); bv = conj(bv); }
     return mk(av.x - bv.y, av.y + bv.x);
   };
-  // inverse transform of one (A, B) pair into buf
+  // inverse transform of one (A, B) pair into buf (by the calling team)
   auto inv = [&](cx<T>* buf, const cx<T>* A, bool ma, const cx<T>* B, bool mb) {
-    warp_transform<MX, +1, false>(buf, tw, [&](int n) { return c2r_load(A, ma, B, mb, n); });
+    fused_fft<MX, +1, false, T>(buf, tws, [&](int n) { return c2r_load(A, ma, B, mb, n); }, lane);
   };
   auto clipE = [&](cx<T>* we) {
-    for (int x = lane; x < MX; x += 32) we[x].y = tmax(we[x].y, emin);
-    __syncwarp();
+    for (int x = lane; x < MX; x += TEAM) we[S(x)].y = tmax(we[S(x)].y, emin);
+    team_sync<TEAM>(bar);
   };
   auto xkk = [&](T e) { return tmin(c01 * sqrt(e), xkmax) + nu; };
 
@@ -230,17 +273,17 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
   __syncthreads();
   if (z0 == 1) {
     for (int x = threadIdx.x; x < MX; x += blockDim.x) {
-      cx<T> uv = UVs(s0)[x];
-      UVs(sm1)[x] = zero_cx<T>();
-      WEs(sm1)[x] = mk((T)0, WEs(s0)[x].y);  // w(0) = 0, e(0) = e(1)
+      cx<T> uv = UVs(s0)[S(x)];
+      UVs(sm1)[S(x)] = zero_cx<T>();
+      WEs(sm1)[S(x)] = mk((T)0, WEs(s0)[S(x)].y);  // w(0) = 0, e(0) = e(1)
       T tu, tv;
       wall_stress<T>(wp.w[0], wp, a, 0, uv.x, uv.y, tu, tv);
       carry[x] = mk(tu, tv);
     }
   } else {
     for (int x = threadIdx.x; x < MX; x += blockDim.x) {
-      cx<T> uvm = UVs(sm1)[x], uv0 = UVs(s0)[x], wxy = work[0][x];
-      T xk = xkk(WEs(sm1)[x].y);
+      cx<T> uvm = UVs(sm1)[S(x)], uv0 = UVs(s0)[S(x)], wxy = work[0][S(x)];
+      T xk = xkk(WEs(sm1)[S(x)].y);
       T uz = (uv0.x - uvm.x) * dzm, vz = (uv0.y - uvm.y) * dzm;
       carry[x] = mk(-xk * (uz + wxy.x), -xk * (vz + wxy.y));
     }
@@ -279,8 +322,8 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
           break;
       }
       if (zero) {
-        for (int x = lane; x < MX; x += 32) dst[x] = zero_cx<T>();
-        __syncwarp();
+        for (int x = lane; x < MX; x += TEAM) dst[x] = zero_cx<T>();
+        team_sync<TEAM>(bar);
       } else if (dst) {
         inv(dst, A, ma, B, mb);
         if (ce) clipE(dst);
@@ -288,15 +331,19 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
     }
     __syncthreads();
     // ---- phase II: fluxes (k_flux) ----
+    // the forward transforms of F+iPe and H reuse the z-1 window slots,
+    // whose rows are dead once each point has read them
+    work[4] = UVs(sm1);
+    work[5] = WEs(sm1);
     const bool top = (z == NZ);
     const bool clip = (!top) && f.clipflag[le - 1];
     const T* dEX = reinterpret_cast<const T*>(f.dEX) + ((size_t)(le - 1) * MY + y) * MX;
     const T* dEY = reinterpret_cast<const T*>(f.dEY) + ((size_t)(le - 1) * MY + y) * MX;
     for (int x = threadIdx.x; x < MX; x += blockDim.x) {
-      const cx<T> uvm = UVs(sm1)[x], uv0 = UVs(s0)[x], uv1 = UVs(sp1)[x];
-      const cx<T> wem = WEs(sm1)[x], we0 = WEs(s0)[x], we1 = WEs(sp1)[x];
-      const cx<T> dxv = work[0][x], dyv = work[1][x], wxy = work[2][x];
-      cx<T> exy = top ? zero_cx<T>() : work[3][x];
+      const cx<T> uvm = UVs(sm1)[S(x)], uv0 = UVs(s0)[S(x)], uv1 = UVs(sp1)[S(x)];
+      const cx<T> wem = WEs(sm1)[S(x)], we0 = WEs(s0)[S(x)], we1 = WEs(sp1)[S(x)];
+      const cx<T> dxv = work[0][S(x)], dyv = work[1][S(x)], wxy = work[2][S(x)];
+      cx<T> exy = top ? zero_cx<T>() : work[3][S(x)];
       if (clip) { exy.x += dEX[x]; exy.y += dEY[x]; }
       const cx<T> tprev = carry[x];
       const T U0 = uv0.x, V0 = uv0.y, Um = uvm.x, Vm = uvm.y, U1 = uv1.x, V1 = uv1.y;
@@ -318,8 +365,8 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
       const T A = U0 * U0 + tuu, B = U0 * V0 + tuv, C = V0 * V0 + tvv;
       const T Pu = -((U1 + U0) * W0 - (Um + U0) * Wm) * todzm + (T)a.forcing - (tuw0 - tprev.x) * dzm;
       const T Pv = -((V1 + V0) * W0 - (Vm + V0) * Wm) * todzm - (tvw0 - tprev.y) * dzm;
-      work[0][x] = mk(A, Pu);
-      work[1][x] = mk(B, Pv);
+      work[0][S(x)] = mk(A, Pu);
+      work[1][S(x)] = mk(B, Pv);
       if (!top) {
         const T xkp = xkk(E1);
         const T wz1 = (W1 - W0) * dzm;
@@ -332,12 +379,12 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
         const T H = (T)0.5 * E0 * (V0 + V1) - (T)2 * xk0 * exy.y;
         const T Pe = -(W1 * E1 - Wm * Em) * todzm +
                      ((xkp + xk0) * (E1 - E0) - (xk0 + xkm) * (E0 - Em)) * (T)a.dzm2 - (T)a.ceps * E0 * sqrt(E0);
-        work[2][x] = mk(C, G);
-        work[3][x] = mk(D, Pw);
-        work[4][x] = mk(F, Pe);
-        work[5][x] = mk(H, (T)0);
+        work[2][S(x)] = mk(C, G);
+        work[3][S(x)] = mk(D, Pw);
+        work[4][S(x)] = mk(F, Pe);
+        work[5][S(x)] = mk(H, (T)0);
       } else {
-        work[2][x] = mk(C, (T)0);
+        work[2][S(x)] = mk(C, (T)0);
       }
       carry[x] = mk(tuw0, tvw0);
       const T d = ux + vy + wz0;
@@ -363,11 +410,11 @@ __global__ void __launch_bounds__(192, 1) k_row_fused(FusedArgs f, StageArgs a, 
     // ---- phase III: forward transforms, -d/dx, truncation to kx < nx/2 ----
     if (!(top && warp >= 3)) {
       cx<T>* buf = work[warp];
-      warp_transform<MX, -1, true>(buf, tw, NoLoad{});
+      fused_fft<MX, -1, true, T>(buf, tws, NoLoad{}, lane);
       const size_t orow = ((size_t)(z - 1) * MY + y) * KX;
       auto O = [&](int j) { return reinterpret_cast<cx<T>*>(f.out.p[j]) + orow; };
-      for (int k = lane; k < KX; k += 32) {
-        cx<T> zk = buf[k], zmr = conj(buf[(MX - k) % MX]);
+      for (int k = lane; k < KX; k += TEAM) {
+        cx<T> zk = buf[S(k)], zmr = conj(buf[S((MX - k) % MX)]);
         cx<T> ah = (zk + zmr) * (T)0.5;
         cx<T> dd = zk - zmr;
         cx<T> bh = mk(dd.y * (T)0.5, -dd.x * (T)0.5);
