@@ -54,7 +54,7 @@ __device__ __forceinline__ void warp_fft(cx<T>* buf, const cx<T>* twn, LoadF loa
       Dft<N1, S, T>::run(v);
 #pragma unroll
       for (int k1 = 0; k1 < N1; k1++) {
-        cx<T> w = twn[lane * k1];
+        cx<T> w = twn[k1 * N2 + lane];  // [k1][n2] layout: consecutive lanes, no bank conflicts
         if (S > 0) w.y = -w.y;
         buf[k1 * LD + lane] = (k1 == 0) ? v[k1] : cmul(v[k1], w);
       }
@@ -103,7 +103,7 @@ __device__ __forceinline__ void team_stockham_pass(cx<T>* buf, const cx<T>* twn,
         if constexpr (FIRST) x = load(j + r * M);
         else x = buf[Swz<T, N>::f(j + r * M)];
         if (NS > 1 && r > 0) {
-          cx<T> w = twn[k * r * (N / (NS * R))];
+          cx<T> w = twn[r * NS + k];  // this pass's table, [r][k] layout
           if (S > 0) w.y = -w.y;
           x = cmul(x, w);
         }
@@ -139,9 +139,27 @@ template <int N, int S, bool IN_SMEM, int TEAM, class T, class LoadF>
 __device__ __forceinline__ void team_fft(cx<T>* buf, const cx<T>* twn, LoadF load, int tl, int bar) {
   constexpr int R1 = Radix3<N>::R1, R2 = Radix3<N>::R2, R3 = Radix3<N>::R3;
   static_assert(R1 * R2 * R3 == N, "radices must multiply to N");
+  // twn: the per-pass tables of stockham_twiddles (pass 2 at 0, pass 3 at R1*R2)
   team_stockham_pass<N, R1, 1, S, !IN_SMEM, TEAM, T>(buf, twn, load, tl, bar);
   team_stockham_pass<N, R2, R1, S, false, TEAM, T>(buf, twn, load, tl, bar);
-  team_stockham_pass<N, R3, R1 * R2, S, false, TEAM, T>(buf, twn, load, tl, bar);
+  team_stockham_pass<N, R3, R1 * R2, S, false, TEAM, T>(buf, twn + R1 * R2, load, tl, bar);
+}
+// Entries of the per-pass twiddle tables used by team_fft: pass 2 (NS = R1,
+// radix R2) then pass 3 (NS = R1*R2, radix R3), each as [r][k] with entry
+// W_N^(k*r*N/(NS*R)).  Returns the length of the table (R1*R2 + R1*R2*R3).
+template <int N> __host__ __device__ constexpr int stockham_twiddle_len() {
+  return Radix3<N>::R1 * Radix3<N>::R2 + N;
+}
+// exponent (in units of 2 pi / N) of entry i of the table
+template <int N> __device__ __forceinline__ int stockham_twiddle_exp(int i) {
+  constexpr int R1 = Radix3<N>::R1, R2 = Radix3<N>::R2, R3 = Radix3<N>::R3;
+  if (i < R1 * R2) {
+    const int r = i / R1, k = i % R1;  // NS = R1, R = R2
+    return k * r * (N / (R1 * R2));
+  }
+  i -= R1 * R2;
+  const int r = i / (R1 * R2), k = i % (R1 * R2);  // NS = R1*R2, R = R3
+  return k * r * (N / (R1 * R2 * R3));
 }
 
 // Transform used by the fused kernel for a (length, type): the two-pass
@@ -178,7 +196,7 @@ template <int NSX> struct FusedCfg {
   template <class T> static constexpr int buf() { return FusedPlan<MX, T>::BUF; }
   // buffers + the twiddle table of length MX staged in shared memory
   template <class T> static constexpr size_t smem() {
-    return ((size_t)NBUF * buf<T>() + MX) * sizeof(cx<T>);
+    return ((size_t)NBUF * buf<T>() + MX + 64) * sizeof(cx<T>);
   }
 };
 
@@ -191,10 +209,20 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   constexpr int TEAM = FusedCfg<NSX>::TEAM;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-  // twiddles exp(-2 pi i j / MX) staged once per CTA: every transform pass
-  // reads them from shared memory instead of the global table
+  // twiddles staged once per CTA in the layout each transform reads with
+  // consecutive lanes: [k1][n2] (two-pass) or the per-pass [r][k] tables
+  // (three-pass Stockham)
   cx<T>* tws = sm + (size_t)11 * BUF;
-  for (int j = threadIdx.x; j < MX; j += blockDim.x) tws[j] = tw[tw_off(MX) + j];
+  {
+    const cx<T>* twg = tw + tw_off(MX);
+    if constexpr (FusedPlan<MX, T>::three) {
+      for (int i = threadIdx.x; i < stockham_twiddle_len<MX>(); i += blockDim.x)
+        tws[i] = twg[stockham_twiddle_exp<MX>(i) % MX];
+    } else {
+      constexpr int N1 = Split<MX>::N1, N2 = Split<MX>::N2;
+      for (int i = threadIdx.x; i < N1 * N2; i += blockDim.x) tws[i] = twg[(i / N2) * (i % N2)];
+    }
+  }
   __syncthreads();
   cx<T>* work[6];
 #pragma unroll
