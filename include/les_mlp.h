@@ -1,0 +1,86 @@
+/*
+ * les_mlp.h -- C ABI of the learned sub-grid closure: a per-point multilayer
+ * perceptron evaluated and trained on the sm_100a tensor cores.
+ *
+ * The closure has no counterpart in the reference: it replaces the eddy
+ * viscosity of complen.f90:69-96 and the stresses of compsgs1.f90:104-156
+ * (tau_ij = -2 nu_t S_ij) with tau_ij predicted from the local resolved
+ * velocity gradients.  The solver uses it when its configuration has
+ * imodel = LES_SGS_LEARNED (les_gpu.h) and a network is attached with
+ * les_gpu_set_mlp; stages whose plane-averaged dissipation
+ * -<tau_ij S_ij> comes out negative fall back to the Deardorff stresses.
+ *
+ * Network: 11 -> 64 -> 64 -> 64 -> 6, GELU (tanh form) after the hidden
+ * layers, bf16 weights and activations, f32 accumulation.
+ *   inputs  f = (ux, vx, wx, uy, vy, wy, uz, vz, wz) * Delta, z+, Delta
+ *           normalised as x_j = (f_j - in_shift_j) * in_scale_j
+ *   outputs y -> tau = y * out_scale + out_shift for
+ *           (tau11, tau22, tau33, tau12, tau13, tau23)
+ * Parameters (LES_MLP_NPARAM floats, this order):
+ *   W1[64][11], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], W4[6][64], b4[6]
+ * Normalisation (LES_MLP_NNORM floats):
+ *   in_shift[11], in_scale[11], out_scale[6], out_shift[6]
+ *
+ * Operator entry points take device pointers and a CUDA stream (NULL = the
+ * legacy default stream); they return 0 or an LES_E* code of les_gpu.h.
+ */
+#ifndef LES_MLP_H
+#define LES_MLP_H
+
+#include "les_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LES_MLP_NIN    11
+#define LES_MLP_NHID   64
+#define LES_MLP_NOUT   6
+#define LES_MLP_NPARAM 9478
+#define LES_MLP_NNORM  34
+/* Sample layouts on the device: features bf16 [n][16] (normalised, columns
+ * 11..15 zero), outputs and targets f32 [n][8] (columns 6, 7 unused). */
+#define LES_MLP_FEAT_STRIDE 16
+#define LES_MLP_OUT_STRIDE  8
+
+typedef struct les_mlp les_mlp;
+
+int les_mlp_create(int device, les_mlp** out);
+void les_mlp_destroy(les_mlp* m);
+const char* les_mlp_last_error(const les_mlp* m);
+
+/* Host arrays: params[LES_MLP_NPARAM], norm[LES_MLP_NNORM].  Setting the
+ * parameters also resets the optimiser state. */
+int les_mlp_set_params(les_mlp* m, const float* params, const float* norm);
+int les_mlp_get_params(les_mlp* m, float* params, float* norm);
+
+/* y[n][8] = network(feat[n][16]) in normalised units (asynchronous). */
+int les_mlp_forward(les_mlp* m, const void* feat, long long n, float* y, void* stream);
+
+/* Mean-squared error over the n samples and 6 outputs, and its gradient
+ * grad[LES_MLP_NPARAM] (device, flat parameter order).  Synchronous. */
+int les_mlp_loss_grad(les_mlp* m, const void* feat, const float* target, long long n, float* grad, double* loss,
+                      void* stream);
+
+/* One Adam step (Kingma & Ba 2015; beta1 0.9, beta2 0.999, eps 1e-8, bias
+ * corrected) on f32 master parameters from the gradient of the batch; the
+ * bf16 copies used by the kernels are refreshed.  *loss (optional) receives
+ * the batch loss before the step, which makes the call synchronous. */
+int les_mlp_adam_step(les_mlp* m, const void* feat, const float* target, long long n, float lr, double* loss,
+                      void* stream);
+
+/* Attach (or with m == NULL detach) a network to a solver handle whose
+ * configuration has imodel = LES_SGS_LEARNED.  re_tau sets the z+ feature.
+ * The handle keeps a reference to m: destroy the handle first. */
+int les_gpu_set_mlp(les_handle* h, les_mlp* m, double re_tau);
+
+/* After a synchronising call: 1 if the last stage used the network (0 if
+ * it fell back to the Deardorff stresses) and that stage's plane-averaged
+ * dissipation -<tau_ij S_ij> of the network's stresses. */
+int les_gpu_learned_status(les_handle* h, int* used, double* dissipation);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LES_MLP_H */

@@ -103,6 +103,17 @@ def lib():
         L.orc_dft.argtypes = [D, ctypes.c_int, ctypes.c_int]
         L.orc_tridv.argtypes = [D, ctypes.c_int, ctypes.c_int]
         L.orc_threads.restype = ctypes.c_int
+        LL = ctypes.c_longlong
+        L.orc_mlp_nparam.restype = ctypes.c_int
+        L.orc_mlp_forward.argtypes = [D, D, LL, D, ctypes.c_int]
+        L.orc_mlp_loss_grad.restype = ctypes.c_double
+        L.orc_mlp_loss_grad.argtypes = [D, D, D, LL, D]
+        L.orc_mlp_loss.restype = ctypes.c_double
+        L.orc_mlp_loss.argtypes = [D, D, D, LL]
+        L.orc_mlp_adam.argtypes = [D, D, D, D, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.orc_bf16_round.restype = ctypes.c_double
+        L.orc_bf16_round.argtypes = [ctypes.c_double]
         _lib = L
     return _lib
 
@@ -258,3 +269,68 @@ def tridv(bdar):
     _, n, ny = b.shape
     lib().orc_tridv(_ptr(b), ny, n)
     return b
+
+
+# ---- learned SGS closure: the FP64 multilayer perceptron (mlp_oracle.h) ----
+MLP_NIN, MLP_NHID, MLP_NOUT, MLP_NPARAM = 11, 64, 6, 9478
+MLP_NNORM = 2 * MLP_NIN + 2 * MLP_NOUT
+
+
+def mlp_slices():
+    """Offsets of W1, b1, W2, b2, W3, b3, W4, b4 in the flat parameter vector."""
+    shapes = [(64, 11), (64,), (64, 64), (64,), (64, 64), (64,), (6, 64), (6,)]
+    out, o = [], 0
+    for sh in shapes:
+        n = int(np.prod(sh))
+        out.append((o, sh))
+        o += n
+    assert o == MLP_NPARAM
+    return out
+
+
+def mlp_init(seed=0, scale=1.0):
+    """Seeded parameters with the variance-preserving scale 1/sqrt(fan_in)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(MLP_NPARAM)
+    for (o, sh) in mlp_slices():
+        if len(sh) == 2:
+            p[o:o + sh[0] * sh[1]] = rng.standard_normal(sh[0] * sh[1]) * scale / np.sqrt(sh[1])
+        else:
+            p[o:o + sh[0]] = rng.standard_normal(sh[0]) * 0.1 * scale
+    return p
+
+
+def mlp_forward(params, x, bf16=False):
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[0]
+    y = np.zeros((n, MLP_NOUT))
+    lib().orc_mlp_forward(_ptr(params), _ptr(x), n, _ptr(y), int(bf16))
+    return y
+
+
+def mlp_loss_grad(params, x, t):
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    g = np.zeros(MLP_NPARAM)
+    loss = lib().orc_mlp_loss_grad(_ptr(params), _ptr(x), _ptr(t), x.shape[0], _ptr(g))
+    return loss, g
+
+
+def mlp_loss(params, x, t):
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    return lib().orc_mlp_loss(_ptr(params), _ptr(np.ascontiguousarray(x, dtype=np.float64)),
+                              _ptr(np.ascontiguousarray(t, dtype=np.float64)), x.shape[0])
+
+
+def mlp_adam(params, m, v, g, lr, step, b1=0.9, b2=0.999, eps=1e-8):
+    for a in (params, m, v):
+        assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    lib().orc_mlp_adam(_ptr(params), _ptr(m), _ptr(v), _ptr(g), params.size, lr, b1, b2, eps, step)
+
+
+def bf16_round(a):
+    f = lib().orc_bf16_round
+    return np.vectorize(f, otypes=[np.float64])(np.asarray(a, dtype=np.float64))

@@ -21,6 +21,7 @@
 
 #include "../../include/les_gpu.h"
 #include "les_fused.cuh"
+#include "les_learned.cuh"
 
 namespace les {
 
@@ -144,6 +145,9 @@ struct EngineBase {
   virtual int read_error() = 0;
   virtual cudaStream_t stream() = 0;
   virtual void stage_eager(bool mnout, int istage, double dt) = 0;
+  // learned closure: attach (or with p == nullptr detach) device parameters
+  virtual void set_mlp(const MlpDev* p, double re_tau) = 0;
+  virtual void learned_status(int* used, double* dissipation) = 0;
 };
 
 template <class T>
@@ -177,6 +181,15 @@ struct Engine : EngineBase {
   // staging for transfers (small-grid physical)
   DevBuf<T> phys[4];
   DevBuf<unsigned char> stage_buf;
+  // learned closure (imodel = LES_SGS_LEARNED with a network attached)
+  const MlpDev* mlp = nullptr;
+  double re_tau = 0.0;
+  int nsm = 148;
+  DevBuf<cx<T>> lgy;   // [9][NZ][NY][KX] gradient spectra along x; reused for tau^ [6][...]
+  DevBuf<T> lphys;     // [9][NZ][NY][NX] gradient planes; reused for tau [6][...]
+  DevBuf<uint4> lfeat; // [N][16] bf16 features
+  DevBuf<double> lpart, lstat;
+  DevBuf<int> lflag;
   // derived scalars
   double dz, dzm, dzm2, todzm, kx0, ky0, dsl, ceps, zody;
   // phase of the split entry points: 0 idle, 1 after comp1, 2 after comprhs, 3 after press
@@ -207,7 +220,8 @@ struct Engine : EngineBase {
     for (auto& b : mixed) b.alloc(nmix * NZ);
     // the fused row kernel covers the Deardorff model without the optional
     // production term; Smagorinsky and tke_production use the unfused kernels
-    fused = (c.imodel == LES_SGS_DEARDORFF && c.tke_production == 0);
+    fused = ((c.imodel == LES_SGS_DEARDORFF || c.imodel == LES_SGS_LEARNED) && c.tke_production == 0);
+    LES_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     if (fused) {
       clipflag.alloc(NZ);
       ephys.alloc(pb * NZ); dEX.alloc(pb * NZ); dEY.alloc(pb * NZ);
@@ -235,6 +249,7 @@ struct Engine : EngineBase {
     clipflag.release(); ephys.release(); dEX.release(); dEY.release(); wallpl.release();
     for (auto& b : xout) b.release();
     for (auto& b : phys) b.release();
+    lgy.release(); lphys.release(); lfeat.release(); lpart.release(); lstat.release(); lflag.release();
   }
   cudaStream_t stream() override { return st; }
 
@@ -422,6 +437,7 @@ struct Engine : EngineBase {
       launch(k_y_inverse<T, N>, dim3(cdiv(KX, CM::TC), NZ, 4), dim3(2 * CM::THREADS), 2 * CM::buf(), st, src, dst,
              KX, NZ, (T)ky0, tw);
     });
+    if (learned_on()) learned_pre();
     if (fused) {
       fused_middle(a);
     } else {
@@ -438,6 +454,80 @@ struct Engine : EngineBase {
       launch(k_y_forward<T, N>, dim3(cdiv(KX, C::TC), NZ, 4), dim3(2 * C::THREADS), smem, st, X, rn, KX, NZ, (T)ky0,
              (T)(1.0 / ((double)MX * MY)), tw);
     });
+    if (learned_on()) learned_post(a);
+  }
+
+  // ---- learned closure ----
+  bool learned_on() const { return mlp != nullptr && cfg.imodel == LES_SGS_LEARNED; }
+  void set_mlp(const MlpDev* p, double rt) override {
+    if (p && cfg.imodel != LES_SGS_LEARNED) throw std::invalid_argument("the handle's imodel is not LES_SGS_LEARNED");
+    if (p && !lgy.p) {
+      lgy.alloc(9 * nm * NZ);
+      lphys.alloc(9 * ps * NZ);
+      lfeat.alloc(2 * ps * NZ);
+      lpart.alloc(nsm);
+      lstat.alloc(2);
+      lflag.alloc(1);
+    }
+    mlp = p;
+    re_tau = rt;
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);  // captured with the previous closure
+    graphs.clear();
+    graph_kernels.clear();
+  }
+  void learned_status(int* used, double* dissipation) override {
+    double v[2] = {0.0, 0.0};
+    if (learned_on()) {
+      LES_CUDA(cudaMemcpyAsync(v, lstat.p, sizeof(v), cudaMemcpyDeviceToHost, st));
+      LES_CUDA(cudaStreamSynchronize(st));
+    }
+    if (used) *used = (int)v[1];
+    if (dissipation) *dissipation = v[0];
+  }
+  // gradients -> features -> network -> tau and the fallback flag
+  void learned_pre() {
+    const size_t N = ps * NZ;
+    with_small(NY, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = ColCfg<NN, T>;
+      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC), NZ, 9), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
+             (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)kx0, (T)ky0, (T)dzm, tw);
+    });
+    with_small(NX, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = RowCfg<NN>;
+      const size_t nrows = 9 * (size_t)NZ * NY;
+      launch(k_row_c2r<T, NN>, dim3(cdiv((nrows + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
+             (const cx<T>*)lgy.p, lphys.p, (int)nrows, KX, tw);
+    });
+    const double h = cfg.zl / 2.0;
+    launch(k_lfeat<T>, dim3(cdiv(N, 256)), dim3(256), 0, st, (const T*)lphys.p, lfeat.p, mlp, (long long)N,
+           (long long)ps, (T)dsl, (T)dz, (T)cfg.zl, (T)(re_tau / h));
+    const long long ntiles = ((long long)N + 127) / 128;
+    const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, nsm);
+    MlpOutTau<T> out{lphys.p, (long long)N};
+    launch(k_mlp_infer<MlpOutTau<T>>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, st, mlp,
+           (const uint4*)lfeat.p, (long long)N, out, lpart.p, err.p);
+    launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, 1.0 / ((double)N * dsl), lflag.p,
+           lstat.p);
+  }
+  // tau^ and its divergence into the new tendencies
+  void learned_post(const StageArgs& a) {
+    with_small(NX, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = RowCfg<NN>;
+      const size_t nrows = 6 * (size_t)NZ * NY;
+      launch(k_row_r2c<T, NN>, dim3(cdiv((nrows + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
+             (const T*)lphys.p, lgy.p, (int)nrows, KX, tw);
+    });
+    with_small(NY, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = ColCfg<NN, T>;
+      launch(k_col_small<T, NN, false>, dim3(cdiv(KX, C::TC), 6 * NZ), dim3(C::THREADS), C::buf(), st,
+             (const cx<T>*)lgy.p, lgy.p, KX, (T)(1.0 / ((double)NX * NY)), tw);
+    });
+    launch(k_ldiv<T>, dim3(cdiv(nm, 128), NZ), dim3(128), 0, st, (const cx<T>*)lgy.p, run.p, rvn.p, rwn.p,
+           (const int*)lflag.p, a);
   }
   // Wall-model plane sums from the physical U, V rows of levels 1 and nnz.
   void wall_params_from(const T* U, const T* V, size_t upper_off, const StageArgs& a) {
@@ -483,6 +573,7 @@ struct Engine : EngineBase {
     for (int i = 0; i < 8; i++) { fa.in.p[i] = mixed[i].p; fa.out.p[i] = xout[i].p; }
     fa.dEX = dEX.p; fa.dEY = dEY.p; fa.clipflag = clipflag.p; fa.wp = wp.p;
     fa.divacc = divacc.p; fa.sgsacc = sgsacc.p;
+    fa.lflag = learned_on() ? lflag.p : nullptr;
     int nch = (int)cdiv(8 * 148, MY);
     nch = std::max(1, std::min(nch, NZ / 8 > 0 ? NZ / 8 : 1));
     fa.zchunk = (int)cdiv(NZ, nch);

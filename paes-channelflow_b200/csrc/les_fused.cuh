@@ -185,6 +185,9 @@ struct FusedArgs {
   const WallParams* wp;
   double* divacc;
   double* sgsacc;
+  // learned closure: when lflag is set and *lflag != 0 the interior momentum
+  // stresses are left to the network (the wall-model rows stay)
+  const int* lflag;
   int zchunk;
 };
 
@@ -244,6 +247,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   const T kx0 = (T)a.kx0, dzm = (T)a.dzm, todzm = (T)a.todzm, emin = (T)a.emin;
   const T xkmax = (T)a.xkmax, nu = (T)a.nu, c01 = (T)0.1 * (T)a.dsl;
   const WallParams& wp = *f.wp;
+  const T mom = (f.lflag && f.lflag[0]) ? (T)0 : (T)1;  // weight of the interior momentum stresses
 
   auto mixrow = [&](int j, int z) -> const cx<T>* {
     return reinterpret_cast<const cx<T>*>(f.in.p[j]) + ((size_t)(z - 1) * MY + y) * KX;
@@ -311,7 +315,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   } else {
     for (int x = threadIdx.x; x < MX; x += blockDim.x) {
       cx<T> uvm = UVs(sm1)[S(x)], uv0 = UVs(s0)[S(x)], wxy = work[0][S(x)];
-      T xk = xkk(WEs(sm1)[S(x)].y);
+      T xk = mom * xkk(WEs(sm1)[S(x)].y);
       T uz = (uv0.x - uvm.x) * dzm, vz = (uv0.y - uvm.y) * dzm;
       carry[x] = mk(-xk * (uz + wxy.x), -xk * (vz + wxy.y));
     }
@@ -378,18 +382,18 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
       const T W0 = we0.x, Wm = wem.x, W1 = we1.x, E0 = we0.y, Em = wem.y, E1 = we1.y;
       const T ux = dxv.x, vx = dxv.y, uy = dyv.x, vy = dyv.y;
       const T xkm = xkk(Em), xk0 = xkk(E0);
-      const T s = xkm + xk0;
+      const T s = mom * (xkm + xk0);
       const T tuu = -s * ux, tvv = -s * vy, tuv = -s * (uy + vx) * (T)0.5;
       T tuw0, tvw0;
       if (top) {
         wall_stress<T>(wp.w[1], wp, a, 1, U0, V0, tuw0, tvw0);
       } else {
         const T uz = (U1 - U0) * dzm, vz = (V1 - V0) * dzm;
-        tuw0 = -xk0 * (uz + wxy.x);
-        tvw0 = -xk0 * (vz + wxy.y);
+        tuw0 = -mom * xk0 * (uz + wxy.x);
+        tvw0 = -mom * xk0 * (vz + wxy.y);
       }
       const T wz0 = (W0 - Wm) * dzm;
-      const T tww0 = -(xkm + xk0) * wz0;
+      const T tww0 = -s * wz0;
       const T A = U0 * U0 + tuu, B = U0 * V0 + tuv, C = V0 * V0 + tvv;
       const T Pu = -((U1 + U0) * W0 - (Um + U0) * Wm) * todzm + (T)a.forcing - (tuw0 - tprev.x) * dzm;
       const T Pv = -((V1 + V0) * W0 - (Vm + V0) * Wm) * todzm - (tvw0 - tprev.y) * dzm;
@@ -398,7 +402,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
       if (!top) {
         const T xkp = xkk(E1);
         const T wz1 = (W1 - W0) * dzm;
-        const T tww1 = -(xk0 + xkp) * wz1;
+        const T tww1 = -mom * (xk0 + xkp) * wz1;
         const T D = (T)0.5 * (U0 + U1) * W0 + tuw0;
         const T G = (T)0.5 * (V0 + V1) * W0 + tvw0;
         const T hp = (T)0.5 * (W1 + W0), hm = (T)0.5 * (W0 + Wm);

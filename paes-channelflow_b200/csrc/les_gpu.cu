@@ -10,7 +10,13 @@
 #include <string>
 #include <thread>
 
+#include "../../include/les_mlp.h"
 #include "les_engine.cuh"
+
+namespace les {
+const MlpDev* mlp_dev_params(const les_mlp* m);
+int mlp_device(const les_mlp* m);
+}  // namespace les
 
 namespace les {
 
@@ -142,6 +148,10 @@ int check_config(const les_config* c, std::string& why) {
     return LES_EINVAL;
   }
   if (c->isurface < 1 || c->isurface > 6) { why = "isurface must be 1..6"; return LES_EINVAL; }
+  if (c->imodel == LES_SGS_LEARNED && c->tke_production) {
+    why = "the learned closure keeps the shipped TKE equation (tke_production = 0)";
+    return LES_EINVAL;
+  }
   if (c->precision != LES_PREC_FP64 && c->precision != LES_PREC_MIXED) {
     why = "precision must be 8 (FP64) or 4 (mixed)";
     return LES_EINVAL;
@@ -336,6 +346,7 @@ int les_gpu_sync(les_handle* h, double timeout_s) {
   if (rc) return rc;
   if (flags & ERR_UTAU) { h->err = "stop because utau > 10 (wall model blow-up guard)"; return LES_EUTAU; }
   if (flags & ERR_NAN) { h->err = "NaN/Inf in the state"; return LES_ENAN; }
+  if (flags & ERR_MMA_TIMEOUT) { h->err = "a tensor-core MMA did not complete within its wait limit"; return LES_ETIMEOUT; }
   return LES_OK;
 }
 
@@ -447,3 +458,19 @@ int les_op_tridv(void* bdar, int ny, int n, int real_bytes, void* stream) {
 }
 
 }  // extern "C"
+
+// ---- learned closure (les_mlp.h) ----
+extern "C" int les_gpu_set_mlp(les_handle* h, les_mlp* m, double re_tau) {
+  if (!h) return LES_EINVAL;
+  if (m) {
+    if (h->cfg.imodel != LES_SGS_LEARNED) { h->err = "les_gpu_set_mlp: imodel is not LES_SGS_LEARNED"; return LES_EINVAL; }
+    if (les::mlp_device(m) != h->device) { h->err = "les_gpu_set_mlp: network and handle on different devices"; return LES_EINVAL; }
+    if (!(re_tau > 0)) { h->err = "les_gpu_set_mlp: re_tau must be positive"; return LES_EINVAL; }
+  }
+  return guarded(h, [&] { h->eng->set_mlp(m ? les::mlp_dev_params(m) : nullptr, re_tau); });
+}
+
+extern "C" int les_gpu_learned_status(les_handle* h, int* used, double* dissipation) {
+  if (!h) return LES_EINVAL;
+  return guarded(h, [&] { h->eng->learned_status(used, dissipation); });
+}

@@ -1,0 +1,173 @@
+// les_learned.cuh -- kernels of the learned sub-grid closure inside the RK3
+// stage (imodel = LES_SGS_LEARNED).
+//
+// The network is evaluated at the cell centres of the physical (unpadded)
+// grid.  Per stage:
+//   1. k_lgrad_y: y-inverse transforms of the nine velocity-gradient spectra
+//      at every level (x-spectral, y-physical), with the level combinations
+//      of the staggered grid applied in spectral space:
+//        ux, vx = i kx u^, i kx v^;  uy, vy = i ky u^, i ky v^
+//        wx, wy = i k (w^(k) + w^(k-1)) / 2        (w-levels k-1, k; w(0) = w(nnz) = 0)
+//        wz     = (w^(k) - w^(k-1)) / dz
+//        uz, vz = (u^(k+1) - u^(k-1)) / (2 dz), one-sided at k = 1 and nnz
+//                 (the centred average of the w-level differences with
+//                  UZ(0) = UZ(1) and UZ(nnz) = UZ(nnz-1), as derivs1.f90 /
+//                  derivs2.f90 set the wall rows)
+//   2. k_row_c2r along x (shared with the rest of the stage);
+//   3. k_lfeat: normalised bf16 features;
+//   4. k_mlp_infer<MlpOutTau>: tau_ij on the tensor cores, and the per-CTA
+//      sums of the dissipation -tau_ij S_ij;
+//   5. k_learned_flag: plane-and-level mean of the dissipation (FP64, fixed
+//      order); flag = 1 when it is >= 0, else 0 (Deardorff fallback);
+//   ... the padded-grid kernels (their interior momentum stresses are
+//      multiplied by 1 - flag) ...
+//   6. k_row_r2c + k_col_small: tau^ at every level;
+//   7. k_ldiv: the stress divergence added to the new tendencies (when flag):
+//        ru += -i kx tau11^ - i ky tau12^ - (tau13w^(k) - tau13w^(k-1)) / dz
+//        rv += -i kx tau12^ - i ky tau22^ - (tau23w^(k) - tau23w^(k-1)) / dz
+//        rw += -i kx tau13w^ - i ky tau23w^ - (tau33^(k+1) - tau33^(k)) / dz   (w-levels)
+//      with tau13w(k) = (tau13(k) + tau13(k+1)) / 2 on interior w-levels and 0
+//      on the walls (the wall model's stresses stay in the padded kernels).
+// The kinetic-energy equation keeps the Deardorff eddy diffusivity.
+#pragma once
+#include "les_kernels.cuh"
+#include "les_mlp.cuh"
+
+namespace les {
+
+// Feature order: (ux, vx, wx, uy, vy, wy, uz, vz, wz) = plane j of the
+// gradient planes, then z+, then Delta.
+template <class T, int N>
+__global__ void __launch_bounds__(ColCfg<N, T>::THREADS)
+k_lgrad_y(const cx<T>* __restrict__ uh, const cx<T>* __restrict__ vh, const cx<T>* __restrict__ wh,
+          cx<T>* __restrict__ gy, int KX, int NZ, T kx0, T ky0, T dzm, const cx<T>* __restrict__ tw) {
+  using C = ColCfg<N, T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+  const int z = blockIdx.y + 1;  // cell centre 1..NZ
+  const int f = blockIdx.z;      // feature plane 0..8
+  const int c0 = blockIdx.x * C::TC;
+  const size_t nm = (size_t)N * KX;
+  auto at = [&](const cx<T>* a, int k, size_t o) -> cx<T> { return a[(size_t)(k - 1) * nm + o]; };
+  auto wl = [&](int k, size_t o) -> cx<T> {  // w-level k, zero on the walls
+    return (k >= 1 && k <= NZ - 1) ? at(wh, k, o) : zero_cx<T>();
+  };
+  fft_core<N, +1, true, false, false>(C::TC, sm, tw, [&](int t, int n) -> cx<T> {
+    const int kx = c0 + t;
+    if (kx >= KX || n == N / 2) return zero_cx<T>();
+    const size_t o = (size_t)n * KX + kx;
+    const T xk = kx0 * (T)kx, yk = ky0 * (T)signed_k(n, N);
+    switch (f) {
+      case 0: return mul_i(at(uh, z, o)) * xk;
+      case 1: return mul_i(at(vh, z, o)) * xk;
+      case 2: return mul_i(wl(z, o) + wl(z - 1, o)) * ((T)0.5 * xk);
+      case 3: return mul_i(at(uh, z, o)) * yk;
+      case 4: return mul_i(at(vh, z, o)) * yk;
+      case 5: return mul_i(wl(z, o) + wl(z - 1, o)) * ((T)0.5 * yk);
+      case 6:
+      case 7: {
+        const cx<T>* a = (f == 6) ? uh : vh;
+        if (z == 1) return (at(a, 2, o) - at(a, 1, o)) * dzm;
+        if (z == NZ) return (at(a, NZ, o) - at(a, NZ - 1, o)) * dzm;
+        return (at(a, z + 1, o) - at(a, z - 1, o)) * ((T)0.5 * dzm);
+      }
+      default: return (wl(z, o) - wl(z - 1, o)) * dzm;
+    }
+  }, [&](int t, int k, cx<T> v) {
+    const int kx = c0 + t;
+    if (kx < KX) gy[((size_t)f * NZ + (z - 1)) * nm + (size_t)k * KX + kx] = v;
+  });
+}
+
+// Normalised bf16 features [N][16] from the nine gradient planes [9][N].
+template <class T>
+__global__ void k_lfeat(const T* __restrict__ g, uint4* __restrict__ feat, const MlpDev* __restrict__ P, long long N,
+                        long long plane, T delta, T dz, T zl, T zplus_per_len) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int z = (int)(p / plane);
+  const T zc = ((T)z + (T)0.5) * dz;
+  const T zw = zc < zl - zc ? zc : zl - zc;
+  float f[16];
+#pragma unroll
+  for (int j = 0; j < 9; j++) f[j] = (float)((g[(size_t)j * N + p] * delta - (T)P->in_shift[j]) * (T)P->in_scale[j]);
+  f[9] = (float)((zw * zplus_per_len - (T)P->in_shift[9]) * (T)P->in_scale[9]);
+  f[10] = (float)((delta - (T)P->in_shift[10]) * (T)P->in_scale[10]);
+#pragma unroll
+  for (int j = 11; j < 16; j++) f[j] = 0.f;
+  feat[2 * p] = make_uint4(pack_bf2(f[0], f[1]), pack_bf2(f[2], f[3]), pack_bf2(f[4], f[5]), pack_bf2(f[6], f[7]));
+  feat[2 * p + 1] = make_uint4(pack_bf2(f[8], f[9]), pack_bf2(f[10], 0.f), 0u, 0u);
+}
+
+__device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
+
+// Network outputs -> tau planes [6][N] (tau11, tau22, tau33, tau12, tau13,
+// tau23) and the dissipation -tau_ij S_ij * Delta from the features.
+template <class T> struct MlpOutTau {
+  T* tau;
+  long long N;
+  __device__ double operator()(long long p, bool valid, const float (&y)[16], uint4 f0, uint4 f1,
+                               const MlpDev* P) const {
+    if (!valid) return 0.0;
+    float t[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+      t[i] = y[i] * P->out_scale[i] + P->out_shift[i];
+      tau[(size_t)i * N + p] = (T)t[i];
+    }
+    const float q[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
+                        bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
+    float g[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) g[j] = q[j] / P->in_scale[j] + P->in_shift[j];  // d_i u_j * Delta
+    // g = (ux, vx, wx, uy, vy, wy, uz, vz, wz) * Delta
+    const float s11 = g[0], s22 = g[4], s33 = g[8];
+    const float s12 = 0.5f * (g[3] + g[1]), s13 = 0.5f * (g[6] + g[2]), s23 = 0.5f * (g[7] + g[5]);
+    return -((double)t[0] * s11 + (double)t[1] * s22 + (double)t[2] * s33 +
+             2.0 * ((double)t[3] * s12 + (double)t[4] * s13 + (double)t[5] * s23));
+  }
+};
+
+// Mean dissipation (per-CTA sums in CTA order) -> flag and status.
+static __global__ void k_learned_flag(const double* __restrict__ part, int nparts, double inv_n_delta,
+                                      int* __restrict__ flag, double* __restrict__ status) {
+  if (threadIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 0; i < nparts; i++) s += part[i];
+  const double mean = s * inv_n_delta;
+  const int use = (mean >= 0.0) ? 1 : 0;  // NaN -> fallback
+  flag[0] = use;
+  status[0] = mean;
+  status[1] = (double)use;
+}
+
+// Stress divergence of the network's tau (spectral, all levels) into the
+// new tendencies, when the stage uses the network.
+template <class T>
+__global__ void k_ldiv(const cx<T>* __restrict__ th, cx<T>* __restrict__ run, cx<T>* __restrict__ rvn,
+                       cx<T>* __restrict__ rwn, const int* __restrict__ flag, StageArgs a) {
+  if (!flag[0]) return;
+  const int KX = a.KX, NY = a.NY, NZ = a.NZ;
+  const int nm = KX * NY;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.y + 1;
+  if (m >= nm) return;
+  const int ky = m / KX, kx = m - ky * KX;
+  if (ky == NY / 2) return;
+  const T xk = (T)(a.kx0 * kx), yk = (T)(a.ky0 * signed_k(ky, NY)), dzm = (T)a.dzm;
+  auto tf = [&](int f, int k) -> cx<T> { return th[((size_t)f * NZ + (k - 1)) * nm + m]; };
+  auto t13w = [&](int k) -> cx<T> { return (k >= 1 && k <= NZ - 1) ? (tf(4, k) + tf(4, k + 1)) * (T)0.5 : zero_cx<T>(); };
+  auto t23w = [&](int k) -> cx<T> { return (k >= 1 && k <= NZ - 1) ? (tf(5, k) + tf(5, k + 1)) * (T)0.5 : zero_cx<T>(); };
+  const size_t o = (size_t)(z - 1) * nm + m;
+  const cx<T> du = mul_i(tf(0, z)) * (-xk) - mul_i(tf(3, z)) * yk - (t13w(z) - t13w(z - 1)) * dzm;
+  const cx<T> dv = mul_i(tf(3, z)) * (-xk) - mul_i(tf(1, z)) * yk - (t23w(z) - t23w(z - 1)) * dzm;
+  run[o] = run[o] + du;
+  rvn[o] = rvn[o] + dv;
+  if (z <= NZ - 1) {
+    const cx<T> dw = mul_i(t13w(z)) * (-xk) - mul_i(t23w(z)) * yk - (tf(2, z + 1) - tf(2, z)) * dzm;
+    rwn[o] = rwn[o] + dw;
+  }
+}
+
+}  // namespace les

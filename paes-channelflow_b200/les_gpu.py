@@ -121,6 +121,17 @@ def lib():
         "les_op_deal": (I, [VP, I, I, I, I, VP]),
         "les_op_tridv": (I, [VP, I, I, I, VP]),
         "les_op_last_error": (ctypes.c_char_p, []),
+        # learned closure (les_mlp.h)
+        "les_mlp_create": (I, [I, ctypes.POINTER(VP)]),
+        "les_mlp_destroy": (None, [VP]),
+        "les_mlp_last_error": (ctypes.c_char_p, [VP]),
+        "les_mlp_set_params": (I, [VP, VP, VP]),
+        "les_mlp_get_params": (I, [VP, VP, VP]),
+        "les_mlp_forward": (I, [VP, VP, ctypes.c_longlong, VP, VP]),
+        "les_mlp_loss_grad": (I, [VP, VP, VP, ctypes.c_longlong, VP, ctypes.POINTER(D), VP]),
+        "les_mlp_adam_step": (I, [VP, VP, VP, ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(D), VP]),
+        "les_gpu_set_mlp": (I, [H, VP, D]),
+        "les_gpu_learned_status": (I, [H, ctypes.POINTER(I), ctypes.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -133,11 +144,13 @@ def lib():
 
 
 def exported_symbols():
-    """Entry points declared in include/les_gpu.h."""
-    hdr = os.path.join(os.path.dirname(HERE), "include", "les_gpu.h")
+    """Entry points declared in include/les_gpu.h and include/les_mlp.h."""
     import re
-    text = open(hdr).read()
-    return sorted(set(re.findall(r"\b(les_(?:gpu|op)_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    for h in ("les_gpu.h", "les_mlp.h"):
+        text = open(os.path.join(os.path.dirname(HERE), "include", h)).read()
+        names.update(re.findall(r"\b(les_(?:gpu|op|mlp)_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def _ptr(a):
@@ -390,3 +403,91 @@ def tridv(bdar):
     _, n, ny = out.shape
     _op_check(lib().les_op_tridv(out.data_ptr(), ny, n, 8, _stream(out)))
     return out
+
+
+# --- learned closure: the perceptron (les_mlp.h) ---
+MLP_NIN, MLP_NOUT, MLP_NPARAM, MLP_NNORM = 11, 6, 9478, 34
+
+
+class Mlp:
+    """The learned closure's network on one device.  Samples are torch CUDA
+    tensors: features bfloat16 (n, 16) normalised (columns 11..15 zero),
+    outputs / targets float32 (n, 8) (columns 6, 7 unused)."""
+
+    def __init__(self, params=None, norm=None, device=0):
+        h = ctypes.c_void_p()
+        rc = lib().les_mlp_create(device, ctypes.byref(h))
+        if rc != LES_OK:
+            raise LesError(rc, "les_mlp_create failed")
+        self.h = h
+        self.device = device
+        if params is not None:
+            self.set_params(params, norm)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().les_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != LES_OK:
+            raise LesError(rc, lib().les_mlp_last_error(self.h).decode())
+
+    def set_params(self, params, norm=None):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if norm is None:
+            norm = np.concatenate([np.zeros(MLP_NIN), np.ones(MLP_NIN), np.ones(MLP_NOUT), np.zeros(MLP_NOUT)])
+        nm = np.ascontiguousarray(norm, dtype=np.float32)
+        assert p.size == MLP_NPARAM and nm.size == MLP_NNORM
+        self._check(lib().les_mlp_set_params(self.h, p.ctypes.data, nm.ctypes.data))
+
+    def get_params(self):
+        p = np.zeros(MLP_NPARAM, dtype=np.float32)
+        nm = np.zeros(MLP_NNORM, dtype=np.float32)
+        self._check(lib().les_mlp_get_params(self.h, p.ctypes.data, nm.ctypes.data))
+        return p, nm
+
+    def forward(self, feat):
+        import torch
+        n = feat.shape[0]
+        y = torch.empty((n, 8), dtype=torch.float32, device=feat.device)
+        self._check(lib().les_mlp_forward(self.h, feat.data_ptr(), n, y.data_ptr(), _stream(feat)))
+        return y
+
+    def loss_grad(self, feat, target):
+        import torch
+        g = torch.empty(MLP_NPARAM, dtype=torch.float32, device=feat.device)
+        loss = ctypes.c_double()
+        self._check(lib().les_mlp_loss_grad(self.h, feat.data_ptr(), target.data_ptr(), feat.shape[0],
+                                            g.data_ptr(), ctypes.byref(loss), _stream(feat)))
+        return loss.value, g
+
+    def adam_step(self, feat, target, lr=1e-3, want_loss=False):
+        loss = ctypes.c_double()
+        self._check(lib().les_mlp_adam_step(self.h, feat.data_ptr(), target.data_ptr(), feat.shape[0], lr,
+                                            ctypes.byref(loss) if want_loss else None, _stream(feat)))
+        return loss.value if want_loss else None
+
+
+def to_feat(x):
+    """(n, 11) array of normalised features -> bfloat16 (n, 16) CUDA tensor."""
+    import torch
+    x = torch.as_tensor(np.asarray(x), dtype=torch.float32)
+    f = torch.zeros((x.shape[0], 16), dtype=torch.float32)
+    f[:, :MLP_NIN] = x
+    return f.to(torch.bfloat16).cuda()
+
+
+def to_target(t):
+    """(n, 6) array -> float32 (n, 8) CUDA tensor."""
+    import torch
+    t = torch.as_tensor(np.asarray(t), dtype=torch.float32)
+    o = torch.zeros((t.shape[0], 8), dtype=torch.float32)
+    o[:, :MLP_NOUT] = t
+    return o.cuda()
