@@ -35,6 +35,7 @@
 #endif
 
 #include "../include/les_gpu.h"
+#include "mlp_oracle.h"
 
 namespace orc {
 
@@ -340,6 +341,14 @@ struct Les {
   std::vector<std::vector<T>> tauww, tauuw, tauvw;
   std::vector<double> meanbuf;  // (19, nnz) column-major
   Spectral<T> sp;
+  // learned closure (imodel = LES_SGS_LEARNED with a network attached)
+  bool learned = false, mlp_bf16 = true;
+  std::vector<double> mlpP, mlpN;
+  double re_tau = 0.0;
+  int learned_used = 0;
+  double learned_dissip = 0.0;
+  T sgs_mom = (T)1;  // weight of the interior momentum stresses of compsgs1
+  Levels<T> lru, lrv, lrw;
 
   // buffer window offsets: ubuf(-1:2), vbuf(-1:2), wbuf(-2:2), ebuf(-1:1)
   T* UB(int k) { return ubuf[k + 1].data(); }
@@ -669,15 +678,16 @@ struct Les {
   // compsgs1 (compsgs1.f90:104-156), kb = 0.
   void compsgs1(int iz, int j, int jp1, int k, int km1, int l, int lm1, int lp1, int nm1, int n, int np1,
                 int np2) {
+    const T mom = sgs_mom;
     if (iz == 1) {
       complen(lm1, -1, nm1, n);
       complen(l, 0, n, np1);
-      for (size_t i = 0; i < pb; i++) tauww[j][i] = -(XKK[lm1][i] + XKK[l][i]) * WZ[n][i];
+      for (size_t i = 0; i < pb; i++) tauww[j][i] = -mom * (XKK[lm1][i] + XKK[l][i]) * WZ[n][i];
       sufsim(km1);
     }
     if (iz != nnz) complen(lp1, 1, np1, np2);
     for (size_t i = 0; i < pb; i++) {
-      T s = XKK[lm1][i] + XKK[l][i];
+      T s = mom * (XKK[lm1][i] + XKK[l][i]);
       tauuu[i] = -s * UX[n][i];
       tauvv[i] = -s * VY[n][i];
       tauuv[i] = -s * (UY[n][i] + VX[n][i]) * (T)0.5;
@@ -687,9 +697,9 @@ struct Les {
       sufsim_upper(k);
     } else {
       for (size_t i = 0; i < pb; i++) {
-        tauww[jp1][i] = -(XKK[l][i] + XKK[lp1][i]) * WZ[np1][i];
-        tauuw[k][i] = -XKK[l][i] * (UZ[l][i] + WX[l][i]);
-        tauvw[k][i] = -XKK[l][i] * (VZ[l][i] + WY[l][i]);
+        tauww[jp1][i] = -mom * (XKK[l][i] + XKK[lp1][i]) * WZ[np1][i];
+        tauuw[k][i] = -mom * XKK[l][i] * (UZ[l][i] + WX[l][i]);
+        tauvw[k][i] = -mom * XKK[l][i] * (VZ[l][i] + WY[l][i]);
       }
     }
   }
@@ -741,9 +751,116 @@ struct Les {
 
   double& M(int row, int iz) { return meanbuf[(size_t)(iz - 1) * 19 + (row - 1)]; }
 
+  // Learned closure (no reference counterpart; replaces complen/compsgs1's
+  // interior stresses).  Velocity gradients at the cell centres of the small
+  // grid from the stage's start state:
+  //   ux.. = spectral x/y derivatives; wx, wy of (w(k) + w(k-1))/2;
+  //   wz = (w(k) - w(k-1))/dz; uz, vz = centred (u(k+1) - u(k-1))/(2dz),
+  //   one-sided at k = 1 and nnz (derivs1.f90 / derivs2.f90 wall rows);
+  // features (g * dsl, z+, dsl), normalised, through the FP64 network; the
+  // stage uses the network when the mean of -tau_ij S_ij is >= 0, and then
+  // adds the dealiased stress divergence to ru, rv, rw:
+  //   ru += -d/dx tau11 - d/dy tau12 - (tau13w(k) - tau13w(k-1))/dz, ...
+  // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on interior w-levels and 0 on
+  // the walls (the wall model's stresses stay in compsgs1).
+  void learned_prepare() {
+    const int NZ = nnz;
+    std::vector<std::vector<T>> tau((size_t)6 * (NZ + 2), std::vector<T>(ps, (T)0));
+    auto TA = [&](int f, int k) -> std::vector<T>& { return tau[(size_t)f * (NZ + 2) + k]; };
+    std::vector<std::vector<T>> g(9, std::vector<T>(ps));
+    std::vector<T> wc(ps);
+    const double h = (double)zl / 2.0;
+    double dsum_ = 0.0;
+    for (int iz = 1; iz <= NZ; iz++) {
+      sp.xderiv(u.at(iz), g[0].data(), xk.data(), nnx, nny);
+      sp.xderiv(v.at(iz), g[1].data(), xk.data(), nnx, nny);
+      for (size_t q = 0; q < ps; q++) wc[q] = (T)0.5 * (w.at(iz)[q] + w.at(iz - 1)[q]);
+      sp.xderiv(wc.data(), g[2].data(), xk.data(), nnx, nny);
+      sp.yderiv(u.at(iz), g[3].data(), yk.data(), nnx, nny);
+      sp.yderiv(v.at(iz), g[4].data(), yk.data(), nnx, nny);
+      sp.yderiv(wc.data(), g[5].data(), yk.data(), nnx, nny);
+      for (size_t q = 0; q < ps; q++) {
+        for (int c = 0; c < 2; c++) {
+          Levels<T>& a = c == 0 ? u : v;
+          T d;
+          if (iz == 1) d = (a.at(2)[q] - a.at(1)[q]) * dzm;
+          else if (iz == NZ) d = (a.at(NZ)[q] - a.at(NZ - 1)[q]) * dzm;
+          else d = (a.at(iz + 1)[q] - a.at(iz - 1)[q]) * ((T)0.5 * dzm);
+          g[6 + c][q] = d;
+        }
+        g[8][q] = (w.at(iz)[q] - w.at(iz - 1)[q]) * dzm;
+      }
+      const double zc = ((double)iz - 0.5) * (double)dz;
+      const double zw = std::min(zc, (double)zl - zc);
+      MlpTrace tr;
+      for (size_t q = 0; q < ps; q++) {
+        double f[kIn], x[kIn];
+        for (int jj = 0; jj < 9; jj++) f[jj] = (double)(g[jj][q] * dsl);
+        f[9] = zw * re_tau / h;
+        f[10] = (double)dsl;
+        for (int jj = 0; jj < kIn; jj++) x[jj] = (f[jj] - mlpN[jj]) * mlpN[kIn + jj];
+        mlp_forward(mlpP.data(), x, tr, mlp_bf16);
+        double t[kOut];
+        for (int o = 0; o < kOut; o++) {
+          t[o] = tr.y[o] * mlpN[2 * kIn + o] + mlpN[2 * kIn + kOut + o];
+          TA(o, iz)[q] = (T)t[o];
+        }
+        const double s11 = g[0][q], s22 = g[4][q], s33 = g[8][q];
+        const double s12 = 0.5 * ((double)g[3][q] + g[1][q]), s13 = 0.5 * ((double)g[6][q] + g[2][q]),
+                     s23 = 0.5 * ((double)g[7][q] + g[5][q]);
+        dsum_ += -(t[0] * s11 + t[1] * s22 + t[2] * s33 + 2.0 * (t[3] * s12 + t[4] * s13 + t[5] * s23));
+      }
+    }
+    learned_dissip = dsum_ / ((double)ps * NZ);
+    learned_used = learned_dissip >= 0.0 ? 1 : 0;
+    if (!learned_used) return;
+    // stress divergence
+    std::vector<T> t13w_m(ps), t13w_p(ps), t23w_m(ps), t23w_p(ps), f1(ps), f2(ps);
+    auto tw = [&](int f, int k, std::vector<T>& o) {
+      if (k < 1 || k > NZ - 1) { std::fill(o.begin(), o.end(), (T)0); return; }
+      for (size_t q = 0; q < ps; q++) o[q] = (T)0.5 * (TA(f, k)[q] + TA(f, k + 1)[q]);
+    };
+    for (int iz = 1; iz <= NZ; iz++) {
+      tw(4, iz - 1, t13w_m); tw(4, iz, t13w_p); tw(5, iz - 1, t23w_m); tw(5, iz, t23w_p);
+      T* a = lru.at(iz);
+      sp.xderiv(TA(0, iz).data(), f1.data(), xk.data(), nnx, nny);
+      sp.yderiv(TA(3, iz).data(), f2.data(), yk.data(), nnx, nny);
+      for (size_t q = 0; q < ps; q++) a[q] = -f1[q] - f2[q] - (t13w_p[q] - t13w_m[q]) * dzm;
+      sp.deal(a, nnx, nny);
+      a = lrv.at(iz);
+      sp.xderiv(TA(3, iz).data(), f1.data(), xk.data(), nnx, nny);
+      sp.yderiv(TA(1, iz).data(), f2.data(), yk.data(), nnx, nny);
+      for (size_t q = 0; q < ps; q++) a[q] = -f1[q] - f2[q] - (t23w_p[q] - t23w_m[q]) * dzm;
+      sp.deal(a, nnx, nny);
+      a = lrw.at(iz);
+      if (iz <= NZ - 1) {
+        sp.xderiv(t13w_p.data(), f1.data(), xk.data(), nnx, nny);
+        sp.yderiv(t23w_p.data(), f2.data(), yk.data(), nnx, nny);
+        for (size_t q = 0; q < ps; q++) a[q] = -f1[q] - f2[q] - (TA(2, iz + 1)[q] - TA(2, iz)[q]) * dzm;
+        sp.deal(a, nnx, nny);
+      } else {
+        std::fill_n(a, ps, (T)0);
+      }
+    }
+  }
+  void set_mlp(const double* P, const double* N, double rt, bool bf16) {
+    if (!P) { learned = false; return; }
+    mlpP.assign(P, P + kNParam);
+    mlpN.assign(N, N + kNNorm);
+    re_tau = rt;
+    mlp_bf16 = bf16;
+    learned = true;
+    if (lru.data.empty()) { lru.alloc(1, nnz, ps); lrv.alloc(1, nnz, ps); lrw.alloc(1, nnz, ps); }
+  }
+
   // comp1 (comp1.f90:1-188) with istart = 1, iend = nnz, kb = 0.
   void comp1(int it, bool mnout, int istage) {
     (void)it;
+    sgs_mom = (T)1;
+    if (learned) {
+      learned_prepare();
+      if (learned_used) sgs_mom = (T)0;
+    }
     for (int iz = 1; iz <= nnz; iz++) {
       int j = iz % 2 + 1 - 1, jp1 = (iz + 1) % 2 + 1 - 1;
       int k = iz % 2 + 1 - 1, km1 = (iz + 1) % 2 + 1 - 1;
@@ -792,6 +909,11 @@ struct Les {
       compress_to(rubuf.data(), ru.at(iz));
       if (iz != nnz) compress_to(rwbuf.data(), rw.at(iz));
       if (iz != nnz) compress_to(rebuf.data(), re.at(iz));
+      if (learned && learned_used) {
+        for (size_t q = 0; q < ps; q++) { ru.at(iz)[q] += lru.at(iz)[q]; rv.at(iz)[q] += lrv.at(iz)[q]; }
+        if (iz != nnz)
+          for (size_t q = 0; q < ps; q++) rw.at(iz)[q] += lrw.at(iz)[q];
+      }
       if (iz != nnz) {
         T* r = rw.at(iz);
         T mean = (T)(dsum(r, ps) * (double)xym);
@@ -1118,6 +1240,28 @@ void* orc_create(const les_config* cfg, int real_bytes) {
   return h;
 }
 void orc_free(void* hp) { delete (OrcHandle*)hp; }
+
+// Learned closure: attach the FP64 network (NULL params detach).
+int orc_set_mlp(void* hp, const double* params, const double* norm, double re_tau, int bf16) {
+  OrcHandle* h = (OrcHandle*)hp;
+  return guarded(h, [&] { DISPATCH(h, L.set_mlp(params, norm, re_tau, bf16 != 0)); });
+}
+// Stress divergence of the last learned stage, (nnx, nny, nnz) FP64 each.
+int orc_get_learned(void* hp, double* lru, double* lrv, double* lrw) {
+  OrcHandle* h = (OrcHandle*)hp;
+  return guarded(h, [&] {
+    DISPATCH(h, {
+      if (!L.learned) throw std::runtime_error("no network attached");
+      read_levels(L.lru, lru, L.nnx, L.nny, L.nnz, L.nnx);
+      read_levels(L.lrv, lrv, L.nnx, L.nny, L.nnz, L.nnx);
+      read_levels(L.lrw, lrw, L.nnx, L.nny, L.nnz, L.nnx);
+    });
+  });
+}
+void orc_learned_status(void* hp, int* used, double* dissipation) {
+  OrcHandle* h = (OrcHandle*)hp;
+  DISPATCH(h, { if (used) *used = L.learned_used; if (dissipation) *dissipation = L.learned_dissip; });
+}
 const char* orc_error(void* hp) { return ((OrcHandle*)hp)->err.c_str(); }
 
 // Fields as FP64 arrays of (nnx, nny, nnz), levels 1..nnz.

@@ -112,6 +112,9 @@ def lib():
         L.orc_mlp_loss.argtypes = [D, D, D, LL]
         L.orc_mlp_adam.argtypes = [D, D, D, D, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.orc_set_mlp.argtypes = [P, D, D, ctypes.c_double, ctypes.c_int]
+        L.orc_learned_status.argtypes = [P, ctypes.POINTER(ctypes.c_int), D]
+        L.orc_get_learned.argtypes = [P, D, D, D]
         L.orc_bf16_round.restype = ctypes.c_double
         L.orc_bf16_round.argtypes = [ctypes.c_double]
         _lib = L
@@ -196,6 +199,23 @@ class Oracle:
 
     def cfl_dt(self, cfl=0.5):
         return lib().orc_cfl_dt(self.h, cfl)
+
+    def set_mlp(self, params, norm, re_tau, bf16=True):
+        """Attach the learned closure's network (imodel = 5)."""
+        self._mlp_keep = (np.ascontiguousarray(params, dtype=np.float64), np.ascontiguousarray(norm, dtype=np.float64))
+        self._check(lib().orc_set_mlp(self.h, _ptr(self._mlp_keep[0]), _ptr(self._mlp_keep[1]), re_tau, int(bf16)))
+
+    def learned_divergence(self):
+        n = (self.cfg.nnz, self.cfg.nny, self.cfg.nnx)
+        a, b, c = np.zeros(n), np.zeros(n), np.zeros(n)
+        self._check(lib().orc_get_learned(self.h, _ptr(a), _ptr(b), _ptr(c)))
+        return a, b, c
+
+    def learned_status(self):
+        used = ctypes.c_int()
+        d = np.zeros(1)
+        lib().orc_learned_status(self.h, ctypes.byref(used), _ptr(d))
+        return used.value, float(d[0])
 
     def set_dt(self, dt):
         lib().orc_set_dt(self.h, dt)

@@ -271,6 +271,19 @@ class LesGpu:
         dt = self.cfg.dt if dt is None else dt
         self._check(lib().les_gpu_step(self.h, it, int(mnout), dt))
 
+    def set_mlp(self, mlp, re_tau):
+        """Attach the learned closure's network (configuration imodel = 5);
+        mlp=None detaches."""
+        self._mlp = mlp
+        self._check(lib().les_gpu_set_mlp(self.h, mlp.h if mlp is not None else None, re_tau))
+
+    def learned_status(self):
+        """(used, dissipation) of the last stage (synchronising)."""
+        used = ctypes.c_int()
+        d = ctypes.c_double()
+        self._check(lib().les_gpu_learned_status(self.h, ctypes.byref(used), ctypes.byref(d)))
+        return used.value, d.value
+
     def sync(self, timeout_s=60.0):
         self._check(lib().les_gpu_sync(self.h, timeout_s))
 

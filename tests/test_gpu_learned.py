@@ -1,0 +1,104 @@
+"""GPU parity of the RK3 stage with the learned closure (imodel = 5) against
+the oracle's learned stage, through the C ABI.
+
+The network runs in bfloat16 on the tensor cores and the oracle emulates
+the bf16 rounding of inputs, weights and activations, so the two networks'
+stresses agree to about 1%; the learned part of a stage's change is
+dtab1 times the stress divergence, and the tolerance below is 5% of that on
+top of the FP64 (or mixed-form) tolerance of the Deardorff stage.  A stage
+whose network is anti-dissipative must reproduce the Deardorff stage
+bit for bit."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from test_gpu_stage import make_pair, relerr
+
+pytestmark = pytest.mark.gpu
+RE_TAU = 180.0
+
+
+def params():
+    P = O.mlp_init(seed=31).astype(np.float32).astype(np.float64)
+    N = np.concatenate([np.zeros(11), np.full(9, 30.0), [2.0 / RE_TAU, 0.0], np.full(6, 1e-3), np.zeros(6)])
+    return P, N
+
+
+def learned_pair(product, sign, precision=8, nx=32, ny=32, nz=16):
+    o, g, f = make_pair(product, nx, ny, nz, precision=precision, imodel=5, re_tau=RE_TAU)
+    P, N = params()
+    N[22:28] *= sign
+    o.set_mlp(P, N, RE_TAU)
+    m = product.Mlp(P, N)
+    g.set_mlp(m, RE_TAU)
+    return o, g, m, f
+
+
+def dissipative_sign(product):
+    o, g, m, f = learned_pair(product, 1.0)
+    o.stage(0, 0, 1)
+    used, _ = o.learned_status()
+    return 1.0 if used else -1.0
+
+
+@pytest.mark.parametrize("precision", [8, 4])
+def test_learned_stage_matches_oracle(gpu_lib, product, precision):
+    sign = dissipative_sign(product)
+    o, g, m, f = learned_pair(product, sign, precision=precision)
+    o.stage(0, 1, 1)
+    g.stage(0, True, 1)
+    used_o, dis_o = o.learned_status()
+    used_g, dis_g = g.learned_status()
+    assert used_o == 1 and used_g == 1
+    assert abs(dis_g - dis_o) <= 0.05 * abs(dis_o)
+    lru, lrv, lrw = o.learned_divergence()
+    lscale = max(np.abs(lru).max(), np.abs(lrv).max(), np.abs(lrw).max())
+    dtab1 = o.cfg.dt * 8.0 / 15.0
+    fo, fg = o.get_fields(), g.download()
+    to_, tg = o.get_tendencies(), g.download_tendencies()
+    vscale = np.abs(fo["u"]).max()
+    rscale = max(np.abs(to_[k]).max() for k in ("ru", "rv", "rw"))
+    base_f, base_t = (1e-11, 1e-9) if precision == 8 else (2e-5, 2e-4)
+    for k in "uvw":
+        err = np.abs(fg[k] - fo[k]).max()
+        assert err <= 0.05 * dtab1 * lscale + base_f * vscale, (k, err, dtab1 * lscale, vscale)
+    for k in ("ru", "rv", "rw"):
+        err = np.abs(tg[k] - to_[k]).max()
+        assert err <= 0.05 * lscale + base_t * rscale, (k, err, lscale, rscale)
+    assert relerr(fg["e"], fo["e"]) <= (1e-10 if precision == 8 else 1e-4)
+
+
+def test_anti_dissipative_network_reproduces_deardorff(gpu_lib, product):
+    sign = -dissipative_sign(product)
+    o, g, m, f = learned_pair(product, sign)
+    g.stage(0, True, 1)
+    used, dis = g.learned_status()
+    assert used == 0 and dis < 0
+    _, d, _ = make_pair(product, 32, 32, 16, imodel=3, re_tau=RE_TAU)
+    d.stage(0, True, 1)
+    a, b = g.download(), d.download()
+    for k in "uvwep":
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_learned_graph_step_matches_stages(gpu_lib, product):
+    sign = dissipative_sign(product)
+    _, g1, m1, _ = learned_pair(product, sign)
+    _, g2, m2, _ = learned_pair(product, sign)
+    for it in range(2):
+        g1.step(it=it, mnout=False)
+        for s in (1, 2, 3):
+            g2.stage(it, False, s)
+    assert g1.learned_status()[0] == 1
+    a, b = g1.download(), g2.download()
+    for k in "uvwe":
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_set_mlp_rejects_other_closures(gpu_lib, product):
+    _, g, _ = make_pair(product, 16, 16, 8, imodel=3)
+    P, N = params()
+    m = product.Mlp(P, N)
+    with pytest.raises(product.LesError) as ei:
+        g.set_mlp(m, RE_TAU)
+    assert ei.value.code == product.LES_EINVAL
