@@ -79,6 +79,23 @@ int les_gpu_set_mlp(les_handle* h, les_mlp* m, double re_tau);
  * dissipation -<tau_ij S_ij> of the network's stresses. */
 int les_gpu_learned_status(les_handle* h, int* used, double* dissipation);
 
+/* Training data (synchronous; out pointers are device memory).
+ *
+ * les_gpu_learn_filter: explicit filter of the handle's current state onto
+ * the grid (nnx/fxy, nny/fxy, nnz/fz), fz = 1 or 2: box average over the
+ * fine cells in z, box-filter transfer sin(k D/2)/(k D/2) with D the coarse
+ * cell size and truncation to the coarse modes in x and y.  out: 9 planes
+ * of (nnz/fz, nny/fxy, nnx/fxy) doubles, in order u, v (cell centres),
+ * w (coarse w-levels), tau11, tau22, tau33, tau12, tau13, tau23 with
+ * tau_ij = filt(u_i u_j) - filt(u_i) filt(u_j) (w averaged to the centres).
+ *
+ * les_gpu_learned_features: the network's raw inputs at every cell centre
+ * of the current state, f32 [nnx*nny*nnz][16] (columns 0..10 as in the
+ * feature list above, unnormalised; 11..15 zero), computed by the kernels
+ * the learned stage uses. */
+int les_gpu_learn_filter(les_handle* h, int fxy, int fz, double* out);
+int les_gpu_learned_features(les_handle* h, double re_tau, float* feat);
+
 #ifdef __cplusplus
 }
 #endif

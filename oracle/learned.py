@@ -1,0 +1,174 @@
+"""ORACLE (test infrastructure only): numpy restatement of the learned
+closure's grid operations, independent of the C++ oracle's Stockham DFT.
+
+- features(): the network inputs at the cell centres of a state (the
+  gradient stencils of the learned stage: spectral x/y derivatives, w
+  averaged to the centres, centred z differences of u, v that are
+  one-sided at the walls as derivs1.f90 / derivs2.f90 set the wall rows);
+- divergence(): the dealiased stress divergence added to ru, rv, rw;
+- filter_fields(): the explicit filter that makes training data from a
+  fine run (z box average, x-y box-filter transfer with truncation to the
+  coarse modes as in redim.f90:277-318, tau_ij = filt(u_i u_j) -
+  filt(u_i) filt(u_j));
+- mlp(): the network in numpy with bfloat16 rounding of inputs, weights and
+  hidden activations.
+Fields are (nz, ny, nx) arrays (x fastest); w holds w-levels 1..nz with
+w(nz) = 0, and w(0) = 0 below.
+"""
+import numpy as np
+
+from oracle import oracle as O
+
+
+def bf16(a):
+    f = np.asarray(a, dtype=np.float64).astype(np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def mlp(P, x, round_bf16=True):
+    q = bf16 if round_bf16 else (lambda a: np.asarray(a, dtype=np.float64))
+    W = [P[o:o + int(np.prod(sh))].reshape(sh) for (o, sh) in O.mlp_slices()]
+    c, a = np.sqrt(2 / np.pi), 0.044715
+    gelu = lambda z: 0.5 * z * (1 + np.tanh(c * (z + a * z ** 3)))
+    h = q(x)
+    for k in range(3):
+        h = q(gelu(h @ q(W[2 * k]).T + W[2 * k + 1]))
+    return h @ q(W[6]).T + W[7]
+
+
+class Spec:
+    """Spectral x/y derivatives and Nyquist removal on (..., ny, nx) planes."""
+
+    def __init__(self, nx, ny, xl, yl):
+        self.nx, self.ny = nx, ny
+        self.kx = 2 * np.pi / xl * np.arange(nx // 2 + 1)
+        self.ky = 2 * np.pi / yl * np.fft.fftfreq(ny, 1.0 / ny)
+        self.mask = np.ones((ny, nx // 2 + 1))
+        self.mask[:, nx // 2] = 0
+        self.mask[ny // 2, :] = 0
+
+    def dx(self, f):
+        return np.fft.irfft2(np.fft.rfft2(f) * 1j * self.kx * self.mask, s=f.shape[-2:])
+
+    def dy(self, f):
+        return np.fft.irfft2(np.fft.rfft2(f) * 1j * self.ky[:, None] * self.mask, s=f.shape[-2:])
+
+    def deal(self, f):
+        return np.fft.irfft2(np.fft.rfft2(f) * self.mask, s=f.shape[-2:])
+
+
+def _wl(w, k, nz):
+    return w[k - 1] if 1 <= k <= nz - 1 else np.zeros(w.shape[1:])
+
+
+def gradients(u, v, w, xl, yl, zl):
+    """Nine gradient planes per level: (9, nz, ny, nx) in feature order
+    (ux, vx, wx, uy, vy, wy, uz, vz, wz)."""
+    nz, ny, nx = u.shape
+    sp = Spec(nx, ny, xl, yl)
+    dz = zl / nz
+    g = np.zeros((9, nz, ny, nx))
+    for k in range(1, nz + 1):
+        wc = 0.5 * (_wl(w, k, nz) + _wl(w, k - 1, nz))
+        g[0, k - 1], g[1, k - 1], g[2, k - 1] = sp.dx(u[k - 1]), sp.dx(v[k - 1]), sp.dx(wc)
+        g[3, k - 1], g[4, k - 1], g[5, k - 1] = sp.dy(u[k - 1]), sp.dy(v[k - 1]), sp.dy(wc)
+        for c, a in enumerate((u, v)):
+            if k == 1:
+                d = (a[1] - a[0]) / dz
+            elif k == nz:
+                d = (a[nz - 1] - a[nz - 2]) / dz
+            else:
+                d = (a[k] - a[k - 2]) / (2 * dz)
+            g[6 + c, k - 1] = d
+        g[8, k - 1] = (_wl(w, k, nz) - _wl(w, k - 1, nz)) / dz
+    return g
+
+
+def features(u, v, w, xl, yl, zl, re_tau):
+    """Raw network inputs (nz*ny*nx, 11): gradients * Delta, z+, Delta."""
+    nz, ny, nx = u.shape
+    dz = zl / nz
+    dsl = (xl / nx * yl / ny * dz) ** (1.0 / 3.0)
+    g = gradients(u, v, w, xl, yl, zl)
+    zc = (np.arange(nz) + 0.5) * dz
+    zp = np.minimum(zc, zl - zc) * re_tau / (zl / 2)
+    f = np.zeros((nz, ny, nx, 11))
+    for j in range(9):
+        f[..., j] = g[j] * dsl
+    f[..., 9] = zp[:, None, None]
+    f[..., 10] = dsl
+    return f.reshape(-1, 11)
+
+
+def dissipation(g, tau):
+    """Mean of -tau_ij S_ij over all points; g from gradients(), tau (6, ...)
+    in the order tau11, tau22, tau33, tau12, tau13, tau23."""
+    s11, s22, s33 = g[0], g[4], g[8]
+    s12, s13, s23 = 0.5 * (g[3] + g[1]), 0.5 * (g[6] + g[2]), 0.5 * (g[7] + g[5])
+    d = -(tau[0] * s11 + tau[1] * s22 + tau[2] * s33 + 2 * (tau[3] * s12 + tau[4] * s13 + tau[5] * s23))
+    return float(d.mean())
+
+
+def divergence(tau, xl, yl, zl):
+    """Dealiased stress divergence (lru, lrv, lrw), each (nz, ny, nx)."""
+    _, nz, ny, nx = tau.shape
+    sp = Spec(nx, ny, xl, yl)
+    dz = zl / nz
+    tw = lambda f, k: 0.5 * (tau[f, k - 1] + tau[f, k]) if 1 <= k <= nz - 1 else np.zeros((ny, nx))
+    lru = np.zeros((nz, ny, nx)); lrv = np.zeros_like(lru); lrw = np.zeros_like(lru)
+    for k in range(1, nz + 1):
+        t = lambda f: tau[f, k - 1]
+        lru[k - 1] = sp.deal(-sp.dx(t(0)) - sp.dy(t(3)) - (tw(4, k) - tw(4, k - 1)) / dz)
+        lrv[k - 1] = sp.deal(-sp.dx(t(3)) - sp.dy(t(1)) - (tw(5, k) - tw(5, k - 1)) / dz)
+        if k <= nz - 1:
+            lrw[k - 1] = sp.deal(-sp.dx(tw(4, k)) - sp.dy(tw(5, k)) - (tau[2, k] - tau[2, k - 1]) / dz)
+    return lru, lrv, lrw
+
+
+def box_transfer(k, width):
+    a = 0.5 * np.asarray(k, dtype=np.float64) * width
+    out = np.ones_like(a)
+    nz = a != 0
+    out[nz] = np.sin(a[nz]) / a[nz]
+    return out
+
+
+def _filter_xy(q, nxc, nyc, xl, yl):
+    ny, nx = q.shape
+    F = np.fft.rfft2(q) / (nx * ny)
+    kxc = np.arange(nxc // 2)
+    kyc = np.fft.fftfreq(nyc, 1.0 / nyc).astype(int)
+    G = box_transfer(2 * np.pi / xl * kxc, xl / nxc)[None, :] * box_transfer(2 * np.pi / yl * kyc, yl / nyc)[:, None]
+    C = np.zeros((nyc, nxc // 2 + 1), dtype=np.complex128)
+    for i, sk in enumerate(kyc):
+        if i == nyc // 2:
+            continue
+        C[i, :nxc // 2] = F[sk % ny, :nxc // 2] * G[i]
+    return np.fft.irfft2(C * (nxc * nyc), s=(nyc, nxc))
+
+
+def filter_fields(u, v, w, xl, yl, fxy, fz):
+    """(9, nz/fz, ny/fxy, nx/fxy): u, v, w (coarse w-levels), tau11, tau22,
+    tau33, tau12, tau13, tau23."""
+    nz, ny, nx = u.shape
+    nzc, nyc, nxc = nz // fz, ny // fxy, nx // fxy
+    wc = np.stack([0.5 * (_wl(w, k, nz) + _wl(w, k - 1, nz)) for k in range(1, nz + 1)])
+    q = [u, v, wc, u * u, v * v, wc * wc, u * v, u * wc, v * wc]
+    qz = [a.reshape(nzc, fz, ny, nx).mean(axis=1) for a in q]
+    if fz == 2:
+        wst = np.stack([0.25 * _wl(w, 2 * K - 1, nz) + 0.5 * _wl(w, 2 * K, nz) + 0.25 * _wl(w, 2 * K + 1, nz)
+                        for K in range(1, nzc + 1)])
+    else:
+        wst = np.stack([_wl(w, K, nz) for K in range(1, nzc + 1)])
+    qz.append(wst)
+    Q = np.array([[_filter_xy(a[K], nxc, nyc, xl, yl) for K in range(nzc)] for a in qz])
+    out = np.zeros((9, nzc, nyc, nxc))
+    out[0], out[1], out[2] = Q[0], Q[1], Q[9]
+    out[3] = Q[3] - Q[0] ** 2
+    out[4] = Q[4] - Q[1] ** 2
+    out[5] = Q[5] - Q[2] ** 2
+    out[6] = Q[6] - Q[0] * Q[1]
+    out[7] = Q[7] - Q[0] * Q[2]
+    out[8] = Q[8] - Q[1] * Q[2]
+    return out

@@ -148,6 +148,8 @@ struct EngineBase {
   // learned closure: attach (or with p == nullptr detach) device parameters
   virtual void set_mlp(const MlpDev* p, double re_tau) = 0;
   virtual void learned_status(int* used, double* dissipation) = 0;
+  virtual void learned_features(double re_tau, float* feat) = 0;
+  virtual void learn_filter(int fxy, int fz, double* out) = 0;
 };
 
 template <class T>
@@ -190,6 +192,8 @@ struct Engine : EngineBase {
   DevBuf<uint4> lfeat; // [N][16] bf16 features
   DevBuf<double> lpart, lstat;
   DevBuf<int> lflag;
+  DevBuf<T> fscr, fcp;      // filter scratch: z-averaged fine planes, coarse planes
+  DevBuf<cx<T>> fsh, fch;   // filter scratch: fine and coarse spectra
   // derived scalars
   double dz, dzm, dzm2, todzm, kx0, ky0, dsl, ceps, zody;
   // phase of the split entry points: 0 idle, 1 after comp1, 2 after comprhs, 3 after press
@@ -250,6 +254,7 @@ struct Engine : EngineBase {
     for (auto& b : xout) b.release();
     for (auto& b : phys) b.release();
     lgy.release(); lphys.release(); lfeat.release(); lpart.release(); lstat.release(); lflag.release();
+    fscr.release(); fcp.release(); fsh.release(); fch.release();
   }
   cudaStream_t stream() override { return st; }
 
@@ -459,16 +464,18 @@ struct Engine : EngineBase {
 
   // ---- learned closure ----
   bool learned_on() const { return mlp != nullptr && cfg.imodel == LES_SGS_LEARNED; }
+  void learned_alloc() {
+    if (lgy.p) return;
+    lgy.alloc(9 * nm * NZ);
+    lphys.alloc(9 * ps * NZ);
+    lfeat.alloc(2 * ps * NZ);
+    lpart.alloc(nsm);
+    lstat.alloc(2);
+    lflag.alloc(1);
+  }
   void set_mlp(const MlpDev* p, double rt) override {
     if (p && cfg.imodel != LES_SGS_LEARNED) throw std::invalid_argument("the handle's imodel is not LES_SGS_LEARNED");
-    if (p && !lgy.p) {
-      lgy.alloc(9 * nm * NZ);
-      lphys.alloc(9 * ps * NZ);
-      lfeat.alloc(2 * ps * NZ);
-      lpart.alloc(nsm);
-      lstat.alloc(2);
-      lflag.alloc(1);
-    }
+    if (p) learned_alloc();
     mlp = p;
     re_tau = rt;
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);  // captured with the previous closure
@@ -484,9 +491,8 @@ struct Engine : EngineBase {
     if (used) *used = (int)v[1];
     if (dissipation) *dissipation = v[0];
   }
-  // gradients -> features -> network -> tau and the fallback flag
-  void learned_pre() {
-    const size_t N = ps * NZ;
+  // the nine gradient planes at the cell centres (lphys [9][N])
+  void learned_gradients() {
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = ColCfg<NN, T>;
@@ -500,6 +506,66 @@ struct Engine : EngineBase {
       launch(k_row_c2r<T, NN>, dim3(cdiv((nrows + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
              (const cx<T>*)lgy.p, lphys.p, (int)nrows, KX, tw);
     });
+  }
+  // raw (unnormalised) features of the current state, f32 [N][16]
+  void learned_features(double rt, float* feat) override {
+    if (phase != 0) throw std::logic_error("learned_features inside a split comp1..comp2 sequence");
+    learned_alloc();
+    learned_gradients();
+    const size_t N = ps * NZ;
+    launch(k_lfeat_raw<T>, dim3(cdiv(N, 256)), dim3(256), 0, st, (const T*)lphys.p, (float4*)feat, (long long)N,
+           (long long)ps, (T)dsl, (T)dz, (T)cfg.zl, (T)(rt / (cfg.zl / 2.0)));
+  }
+  // explicit filter of the current state onto the grid (NX/fxy, NY/fxy, NZ/fz)
+  void learn_filter(int fxy, int fz, double* out) override {
+    if (phase != 0) throw std::logic_error("learn_filter inside a split comp1..comp2 sequence");
+    if (fxy < 1 || fz < 1 || fz > 2 || NX % fxy || NY % fxy || NZ % fz)
+      throw std::invalid_argument("learn_filter: unsupported filter factors for this grid");
+    const int NXc = NX / fxy, NYc = NY / fxy, NZc = NZ / fz, KXc = NXc / 2;
+    if (!supported_small(NXc) || !supported_small(NYc) || NZc < 4)
+      throw std::invalid_argument("learn_filter: unsupported coarse grid");
+    const size_t npl = (size_t)10 * NZc, psc = (size_t)NXc * NYc, nmc = (size_t)KXc * NYc;
+    if (fscr.n < npl * ps) { fscr.release(); fscr.alloc(npl * ps); }
+    if (fsh.n < npl * nm) { fsh.release(); fsh.alloc(npl * nm); }
+    if (fch.n < npl * nmc) { fch.release(); fch.alloc(npl * nmc); }
+    if (fcp.n < npl * psc) { fcp.release(); fcp.alloc(npl * psc); }
+    to_physical(uh.p, phys[0].p, NZ);
+    to_physical(vh.p, phys[1].p, NZ);
+    to_physical(wh.p, phys[2].p, NZ);
+    launch(k_filt_z<T>, dim3(cdiv(ps, 256), NZc), dim3(256), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
+           (const T*)phys[2].p, fscr.p, (long long)ps, NZ, NZc, fz);
+    with_small(NX, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = RowCfg<NN>;
+      launch(k_row_r2c<T, NN>, dim3(cdiv((npl * NY + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
+             (const T*)fscr.p, fsh.p, (int)(npl * NY), KX, tw);
+    });
+    with_small(NY, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = ColCfg<NN, T>;
+      launch(k_col_small<T, NN, false>, dim3(cdiv(KX, C::TC), (unsigned)npl), dim3(C::THREADS), C::buf(), st,
+             (const cx<T>*)fsh.p, fsh.p, KX, (T)(1.0 / ((double)NX * NY)), tw);
+    });
+    launch(k_filt_trunc<T>, dim3(cdiv(nmc, 256), (unsigned)npl), dim3(256), 0, st, (const cx<T>*)fsh.p, fch.p, NY,
+           KX, NYc, KXc, kx0, ky0, cfg.xl / NXc, cfg.yl / NYc);
+    with_small(NYc, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = ColCfg<NN, T>;
+      launch(k_col_small<T, NN, true>, dim3(cdiv(KXc, C::TC), (unsigned)npl), dim3(C::THREADS), C::buf(), st,
+             (const cx<T>*)fch.p, fch.p, KXc, (T)1, tw);
+    });
+    with_small(NXc, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = RowCfg<NN>;
+      launch(k_row_c2r<T, NN>, dim3(cdiv((npl * NYc + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
+             (const cx<T>*)fch.p, fcp.p, (int)(npl * NYc), KXc, tw);
+    });
+    launch(k_filt_tau<T>, dim3(cdiv(psc * NZc, 256)), dim3(256), 0, st, (const T*)fcp.p, out, (long long)(psc * NZc));
+  }
+  // gradients -> features -> network -> tau and the fallback flag
+  void learned_pre() {
+    const size_t N = ps * NZ;
+    learned_gradients();
     const double h = cfg.zl / 2.0;
     launch(k_lfeat<T>, dim3(cdiv(N, 256)), dim3(256), 0, st, (const T*)lphys.p, lfeat.p, mlp, (long long)N,
            (long long)ps, (T)dsl, (T)dz, (T)cfg.zl, (T)(re_tau / h));

@@ -474,3 +474,20 @@ extern "C" int les_gpu_learned_status(les_handle* h, int* used, double* dissipat
   if (!h) return LES_EINVAL;
   return guarded(h, [&] { h->eng->learned_status(used, dissipation); });
 }
+
+extern "C" int les_gpu_learn_filter(les_handle* h, int fxy, int fz, double* out) {
+  if (!h || !out) return LES_EINVAL;
+  return guarded(h, [&] {
+    h->eng->learn_filter(fxy, fz, out);
+    LES_CUDA(cudaStreamSynchronize(h->eng->stream()));
+  });
+}
+
+extern "C" int les_gpu_learned_features(les_handle* h, double re_tau, float* feat) {
+  if (!h || !feat || !(re_tau > 0)) return LES_EINVAL;
+  if ((uintptr_t)feat % 16) { h->err = "les_gpu_learned_features: feat must be 16-byte aligned"; return LES_EINVAL; }
+  return guarded(h, [&] {
+    h->eng->learned_features(re_tau, feat);
+    LES_CUDA(cudaStreamSynchronize(h->eng->stream()));
+  });
+}

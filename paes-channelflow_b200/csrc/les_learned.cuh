@@ -171,3 +171,103 @@ __global__ void k_ldiv(const cx<T>* __restrict__ th, cx<T>* __restrict__ run, cx
 }
 
 }  // namespace les
+
+namespace les {
+
+// ---------------------------------------------------------------------------
+// Training data of the learned closure: explicit filtering of a fine run.
+// z: box average over the fz fine cells of each coarse cell (fz = 1 or 2);
+// x, y: the box filter of width Delta_c (the coarse cell) as the spectral
+// transfer sin(k Delta_c / 2) / (k Delta_c / 2), then truncation to the
+// coarse modes (|kx| < nxc/2, |ky| < nyc/2; the truncation of redim.f90:
+// 277-318 without its Nyquist rows).  Filtered quantities at the coarse
+// cell centres: u, v, wc, uu, vv, wc wc, u v, u wc, v wc (wc = w averaged to
+// the fine centres), and w at the coarse w-levels (fz = 2: weights 1/4,
+// 1/2, 1/4 of the fine w-levels 2K-1, 2K, 2K+1).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_filt_z(const T* __restrict__ U, const T* __restrict__ V, const T* __restrict__ W,
+                         T* __restrict__ S, long long ps, int NZ, int NZc, int fz) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int K = blockIdx.y + 1;
+  if (p >= ps) return;
+  auto w = [&](int k) -> T { return (k >= 1 && k <= NZ - 1) ? W[(size_t)(k - 1) * ps + p] : (T)0; };
+  T q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int j = 0; j < fz; j++) {
+    const int k = fz * (K - 1) + 1 + j;
+    const T u = U[(size_t)(k - 1) * ps + p], v = V[(size_t)(k - 1) * ps + p];
+    const T wc = (T)0.5 * (w(k) + w(k - 1));
+    q[0] += u; q[1] += v; q[2] += wc;
+    q[3] += u * u; q[4] += v * v; q[5] += wc * wc;
+    q[6] += u * v; q[7] += u * wc; q[8] += v * wc;
+  }
+  const T inv = (T)1 / (T)fz;
+  const size_t plane = (size_t)NZc * ps;
+#pragma unroll
+  for (int i = 0; i < 9; i++) S[i * plane + (size_t)(K - 1) * ps + p] = q[i] * inv;
+  const T wst = (fz == 2) ? (T)0.25 * w(2 * K - 1) + (T)0.5 * w(2 * K) + (T)0.25 * w(2 * K + 1) : w(K);
+  S[9 * plane + (size_t)(K - 1) * ps + p] = wst;
+}
+
+__host__ __device__ inline double box_transfer(double k, double width) {
+  const double a = 0.5 * k * width;
+  return a == 0.0 ? 1.0 : sin(a) / a;
+}
+
+// fine spectra [plane][NY][KX] -> coarse spectra [plane][NYc][KXc]
+template <class T>
+__global__ void k_filt_trunc(const cx<T>* __restrict__ F, cx<T>* __restrict__ C, int NY, int KX, int NYc, int KXc,
+                             double kx0, double ky0, double wx, double wy) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pl = blockIdx.y;
+  if (m >= NYc * KXc) return;
+  const int kyc = m / KXc, kxc = m - kyc * KXc;
+  cx<T> v = zero_cx<T>();
+  if (kyc != NYc / 2) {
+    const int sk = signed_k(kyc, NYc);
+    const int kyf = sk >= 0 ? sk : NY + sk;
+    const double g = box_transfer(kx0 * kxc, wx) * box_transfer(ky0 * sk, wy);
+    v = F[(size_t)pl * NY * KX + (size_t)kyf * KX + kxc] * (T)g;
+  }
+  C[(size_t)pl * NYc * KXc + m] = v;
+}
+
+// coarse filtered planes [10][N] -> out [9][N] (double):
+// u, v, w (w-levels), tau11, tau22, tau33, tau12, tau13, tau23
+template <class T>
+__global__ void k_filt_tau(const T* __restrict__ Q, double* __restrict__ out, long long N) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const double u = Q[p], v = Q[N + p], wc = Q[2 * N + p];
+  out[p] = u;
+  out[N + p] = v;
+  out[2 * N + p] = Q[9 * N + p];
+  out[3 * N + p] = Q[3 * N + p] - u * u;
+  out[4 * N + p] = Q[4 * N + p] - v * v;
+  out[5 * N + p] = Q[5 * N + p] - wc * wc;
+  out[6 * N + p] = Q[6 * N + p] - u * v;
+  out[7 * N + p] = Q[7 * N + p] - u * wc;
+  out[8 * N + p] = Q[8 * N + p] - v * wc;
+}
+
+// raw features f32 [N][16]: 9 gradients * Delta, z+, Delta, zeros
+template <class T>
+__global__ void k_lfeat_raw(const T* __restrict__ g, float4* __restrict__ feat, long long N, long long plane, T delta,
+                            T dz, T zl, T zplus_per_len) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int z = (int)(p / plane);
+  const T zc = ((T)z + (T)0.5) * dz;
+  const T zw = zc < zl - zc ? zc : zl - zc;
+  float f[16];
+#pragma unroll
+  for (int j = 0; j < 9; j++) f[j] = (float)(g[(size_t)j * N + p] * delta);
+  f[9] = (float)(zw * zplus_per_len);
+  f[10] = (float)delta;
+#pragma unroll
+  for (int j = 11; j < 16; j++) f[j] = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; j++) feat[4 * p + j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+}
+
+}  // namespace les

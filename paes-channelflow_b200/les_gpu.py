@@ -132,6 +132,8 @@ def lib():
         "les_mlp_adam_step": (I, [VP, VP, VP, ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(D), VP]),
         "les_gpu_set_mlp": (I, [H, VP, D]),
         "les_gpu_learned_status": (I, [H, ctypes.POINTER(I), ctypes.POINTER(D)]),
+        "les_gpu_learn_filter": (I, [H, I, I, VP]),
+        "les_gpu_learned_features": (I, [H, D, VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -283,6 +285,25 @@ class LesGpu:
         d = ctypes.c_double()
         self._check(lib().les_gpu_learned_status(self.h, ctypes.byref(used), ctypes.byref(d)))
         return used.value, d.value
+
+    def learn_filter(self, fxy, fz):
+        """Filtered coarse fields of the current state: float64 CUDA tensor
+        (9, nnz/fz, nny/fxy, nnx/fxy) = u, v, w, tau11, tau22, tau33, tau12,
+        tau13, tau23."""
+        import torch
+        c = self.cfg
+        out = torch.empty((9, c.nnz // fz, c.nny // fxy, c.nnx // fxy), dtype=torch.float64,
+                          device="cuda:%d" % c.device)
+        self._check(lib().les_gpu_learn_filter(self.h, fxy, fz, out.data_ptr()))
+        return out
+
+    def learned_features(self, re_tau):
+        """Raw network inputs at every cell centre: float32 CUDA tensor (N, 16)."""
+        import torch
+        c = self.cfg
+        out = torch.empty((c.nnx * c.nny * c.nnz, 16), dtype=torch.float32, device="cuda:%d" % c.device)
+        self._check(lib().les_gpu_learned_features(self.h, re_tau, out.data_ptr()))
+        return out
 
     def sync(self, timeout_s=60.0):
         self._check(lib().les_gpu_sync(self.h, timeout_s))

@@ -102,3 +102,29 @@ def test_set_mlp_rejects_other_closures(gpu_lib, product):
     with pytest.raises(product.LesError) as ei:
         g.set_mlp(m, RE_TAU)
     assert ei.value.code == product.LES_EINVAL
+
+
+def test_learn_filter_matches_numpy(gpu_lib, product):
+    from oracle import learned as LN
+    o, g, f = make_pair(product, 64, 64, 16, imodel=3)
+    out = g.learn_filter(4, 2).cpu().numpy()
+    ref = LN.filter_fields(f["u"], f["v"], f["w"], o.cfg.xl, o.cfg.yl, 4, 2)
+    assert out.shape == ref.shape == (9, 8, 16, 16)
+    us = np.abs(f["u"]).max()
+    for i in range(9):
+        tol = 1e-12 * (us if i < 3 else us * us)
+        err = np.abs(out[i] - ref[i]).max()
+        assert err <= tol, (i, err, tol)
+    assert np.abs(ref[3]).max() > 1e-6  # the stresses are not trivially zero
+
+
+def test_learned_features_match_numpy(gpu_lib, product):
+    from oracle import learned as LN
+    o, g, f = make_pair(product, 32, 32, 16, imodel=3)
+    feat = g.learned_features(RE_TAU).cpu().numpy()
+    ref = LN.features(f["u"], f["v"], f["w"], o.cfg.xl, o.cfg.yl, o.cfg.zl, RE_TAU)
+    assert np.all(feat[:, 11:] == 0)
+    for j in range(11):
+        scale = np.abs(ref[:, j]).max()
+        err = np.abs(feat[:, j] - ref[:, j]).max()
+        assert err <= 1e-6 * scale + 1e-30, (j, err, scale)  # f32 output

@@ -1,93 +1,17 @@
 """CPU tests of the oracle's learned closure (les_oracle.cpp learned_prepare)
-against an independent numpy restatement: physical-grid gradients by
-numpy.fft, the network in numpy with the same bfloat16 rounding, the
-dissipation test, and the dealiased stress divergence.  Also: a stage whose
-network is anti-dissipative falls back to the Deardorff stresses exactly."""
+against the independent numpy restatement in oracle/learned.py (gradients
+by numpy.fft, the network in numpy with the same bfloat16 rounding, the
+dissipation test, the dealiased stress divergence), a stage whose network
+is anti-dissipative falling back to the Deardorff stresses exactly, and
+known answers of the training-data filter."""
 import numpy as np
 import pytest
 
+from oracle import learned as LN
 from oracle import oracle as O
 
 NX, NY, NZ = 16, 16, 8
 RE_TAU = 180.0
-
-
-def bf16(a):
-    f = np.asarray(a, dtype=np.float64).astype(np.float32)
-    u = f.view(np.uint32).astype(np.uint64)
-    return ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32).view(np.float32).astype(np.float64)
-
-
-def np_mlp(P, x):
-    sl = O.mlp_slices()
-    W = [P[o:o + int(np.prod(sh))].reshape(sh) for (o, sh) in sl]
-    c, a = np.sqrt(2 / np.pi), 0.044715
-    gelu = lambda z: 0.5 * z * (1 + np.tanh(c * (z + a * z ** 3)))
-    h = bf16(x)
-    for k in range(3):
-        h = bf16(gelu(h @ bf16(W[2 * k]).T + W[2 * k + 1]))
-    return h @ bf16(W[6]).T + W[7]
-
-
-class Spec:
-    def __init__(self, cfg):
-        self.kx = 2 * np.pi / cfg.xl * np.arange(NX // 2 + 1)
-        self.ky = 2 * np.pi / cfg.yl * np.fft.fftfreq(NY, 1.0 / NY)
-        self.mask = np.ones((NY, NX // 2 + 1))
-        self.mask[:, NX // 2] = 0
-        self.mask[NY // 2, :] = 0
-
-    def dx(self, f):
-        return np.fft.irfft2(np.fft.rfft2(f) * 1j * self.kx[None, :] * self.mask, s=f.shape)
-
-    def dy(self, f):
-        return np.fft.irfft2(np.fft.rfft2(f) * 1j * self.ky[:, None] * self.mask, s=f.shape)
-
-    def deal(self, f):
-        return np.fft.irfft2(np.fft.rfft2(f) * self.mask, s=f.shape)
-
-
-def np_learned(cfg, u, v, w, P, N):
-    sp = Spec(cfg)
-    dz = cfg.zl / NZ
-    dsl = (cfg.xl / NX * cfg.yl / NY * dz) ** (1 / 3)
-    wl = lambda k: w[k - 1] if 1 <= k <= NZ - 1 else np.zeros((NY, NX))
-    tau = np.zeros((6, NZ + 2, NY, NX))
-    dis = 0.0
-    for k in range(1, NZ + 1):
-        wc = 0.5 * (wl(k) + wl(k - 1))
-        U = lambda a, kk: a[kk - 1]
-        g = [sp.dx(U(u, k)), sp.dx(U(v, k)), sp.dx(wc), sp.dy(U(u, k)), sp.dy(U(v, k)), sp.dy(wc)]
-        for a in (u, v):
-            if k == 1:
-                g.append((U(a, 2) - U(a, 1)) / dz)
-            elif k == NZ:
-                g.append((U(a, NZ) - U(a, NZ - 1)) / dz)
-            else:
-                g.append((U(a, k + 1) - U(a, k - 1)) / (2 * dz))
-        g.append((wl(k) - wl(k - 1)) / dz)
-        zc = (k - 0.5) * dz
-        zw = min(zc, cfg.zl - zc)
-        f = np.stack([gg.ravel() * dsl for gg in g] + [np.full(NX * NY, zw * RE_TAU / (cfg.zl / 2)),
-                                                       np.full(NX * NY, dsl)], axis=1)
-        x = (f - N[:11]) * N[11:22]
-        y = np_mlp(P, x)
-        t = y * N[22:28] + N[28:34]
-        for i in range(6):
-            tau[i, k] = t[:, i].reshape(NY, NX)
-        s11, s22, s33 = g[0], g[4], g[8]
-        s12, s13, s23 = 0.5 * (g[3] + g[1]), 0.5 * (g[6] + g[2]), 0.5 * (g[7] + g[5])
-        T = [tau[i, k] for i in range(6)]
-        dis += np.sum(-(T[0] * s11 + T[1] * s22 + T[2] * s33 + 2 * (T[3] * s12 + T[4] * s13 + T[5] * s23)))
-    dis /= NX * NY * NZ
-    tw = lambda f, k: 0.5 * (tau[f, k] + tau[f, k + 1]) if 1 <= k <= NZ - 1 else np.zeros((NY, NX))
-    lru = np.zeros((NZ, NY, NX)); lrv = np.zeros_like(lru); lrw = np.zeros_like(lru)
-    for k in range(1, NZ + 1):
-        lru[k - 1] = sp.deal(-sp.dx(tau[0, k]) - sp.dy(tau[3, k]) - (tw(4, k) - tw(4, k - 1)) / dz)
-        lrv[k - 1] = sp.deal(-sp.dx(tau[3, k]) - sp.dy(tau[1, k]) - (tw(5, k) - tw(5, k - 1)) / dz)
-        if k <= NZ - 1:
-            lrw[k - 1] = sp.deal(-sp.dx(tw(4, k)) - sp.dy(tw(5, k)) - (tau[2, k + 1] - tau[2, k]) / dz)
-    return dis, lru, lrv, lrw
 
 
 def make_case(sign):
@@ -97,21 +21,27 @@ def make_case(sign):
     o.dt_used = o.cfl_dt(0.5)
     o.set_dt(o.dt_used)
     fl = o.get_fields()
-    u, v, w = fl["u"], fl["v"], fl["w"]
     P = O.mlp_init(seed=31)
-    N = np.concatenate([np.zeros(11), np.full(9, 30.0), [2.0 / RE_TAU, 1.0], np.full(6, sign * 1e-3), np.zeros(6)])
-    N[21] = 0.0  # Delta is constant on one grid: normalised to zero with scale 0
+    N = np.concatenate([np.zeros(11), np.full(9, 30.0), [2.0 / RE_TAU, 0.0], np.full(6, sign * 1e-3), np.zeros(6)])
     return cfg, o, fl, P, N
+
+
+def np_learned(cfg, fl, P, N):
+    u, v, w = fl["u"], fl["v"], fl["w"]
+    f = LN.features(u, v, w, cfg.xl, cfg.yl, cfg.zl, RE_TAU)
+    y = LN.mlp(P, (f - N[:11]) * N[11:22])
+    tau = (y * N[22:28] + N[28:34]).T.reshape(6, NZ, NY, NX)
+    g = LN.gradients(u, v, w, cfg.xl, cfg.yl, cfg.zl)
+    return LN.dissipation(g, tau), LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl)
 
 
 @pytest.mark.parametrize("sign", [1.0, -1.0])
 def test_learned_prepare_matches_numpy(sign):
     cfg, o, fl, P, N = make_case(sign)
-    u, v, w = fl["u"], fl["v"], fl["w"]
     o.set_mlp(P, N, RE_TAU)
     o.stage(0, 0, 1)
     used, dis = o.learned_status()
-    dis_np, lru, lrv, lrw = np_learned(cfg, u, v, w, P, N)
+    dis_np, (lru, lrv, lrw) = np_learned(cfg, fl, P, N)
     assert abs(dis - dis_np) <= 1e-9 * abs(dis_np)
     assert used == (1 if dis_np >= 0 else 0)
     if used:
@@ -130,7 +60,6 @@ def test_anti_dissipative_network_falls_back_to_deardorff():
         if used:
             continue
         assert dis < 0
-        # same state, Deardorff closure
         cfg3 = O.make_config(NX, NY, NZ, re_tau=RE_TAU, imodel=3)
         d = O.Oracle(cfg3)
         d.set_fields(**fields)
@@ -141,3 +70,47 @@ def test_anti_dissipative_network_falls_back_to_deardorff():
             np.testing.assert_array_equal(a[k], b[k])
         return
     pytest.fail("neither sign gave an anti-dissipative network")
+
+
+def _grid(nx, ny, nz, xl, yl, zl):
+    x = np.arange(nx) * xl / nx
+    y = np.arange(ny) * yl / ny
+    zc = (np.arange(nz) + 0.5) * zl / nz
+    return np.meshgrid(zc, y, x, indexing="ij")
+
+
+def test_filter_transfer_of_single_modes():
+    nx, ny, nz, xl, yl, zl = 32, 32, 8, 2 * np.pi, np.pi, 2.0
+    Z, Y, X = _grid(nx, ny, nz, xl, yl, zl)
+    kx, ky = 3, 2
+    u = np.cos(kx * X) * np.ones_like(Z)
+    v = np.sin(2 * np.pi * ky * Y / yl) * (1 + Z)
+    w = np.zeros_like(u)
+    out = LN.filter_fields(u, v, w, xl, yl, 4, 2)
+    Zc, Yc, Xc = _grid(nx // 4, ny // 4, nz // 2, xl, yl, zl)
+    gx = LN.box_transfer(np.array([kx * 2 * np.pi / xl]), xl / (nx // 4))[0]
+    gy = LN.box_transfer(np.array([ky * 2 * np.pi / yl]), yl / (ny // 4))[0]
+    np.testing.assert_allclose(out[0], gx * np.cos(kx * Xc), atol=1e-13)
+    # z: the pair average of a linear profile is its value at the coarse centre
+    np.testing.assert_allclose(out[1], gy * np.sin(2 * np.pi * ky * Yc / yl) * (1 + Zc), atol=1e-13)
+    # no w: the w stresses vanish
+    for i in (2, 5, 7, 8):
+        assert np.abs(out[i]).max() < 1e-14
+
+
+def test_filter_constants_and_z_box():
+    nx, ny, nz, xl, yl, zl = 32, 32, 8, 2 * np.pi, np.pi, 2.0
+    rng = np.random.default_rng(1)
+    c = rng.standard_normal(3)
+    u = np.full((nz, ny, nx), c[0]); v = np.full_like(u, c[1])
+    w = np.full_like(u, c[2]); w[-1] = 0
+    out = LN.filter_fields(u, v, w, xl, yl, 4, 1)
+    np.testing.assert_allclose(out[0], c[0], atol=1e-14)
+    for i in (3, 4, 6):
+        assert np.abs(out[i]).max() < 1e-13
+    # a field that varies only in z sees only the z box (a positive kernel):
+    # tau11 is the variance of each pair of fine levels
+    uz = rng.standard_normal(nz)
+    u = np.broadcast_to(uz[:, None, None], (nz, ny, nx)).copy()
+    out = LN.filter_fields(u, v, w, xl, yl, 4, 2)
+    np.testing.assert_allclose(out[3][:, 0, 0], 0.25 * (uz[0::2] - uz[1::2]) ** 2, rtol=1e-12)
