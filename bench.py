@@ -1,18 +1,25 @@
 """Benchmark of the LES RK3 hot path (one JSON line on rank 0).
 
 Workload: the production channel grid nx=ny=512, nz=256 (67.1 M points,
-3/2-padded planes of 768x768), Re_tau=590, Deardorff TKE SGS, wall model
-isurface=6, seeded synthetic initial field (parabolic mean + uniform
-perturbations, projected divergence-free) built on the device, fixed dt at
-CFL 0.5.  A step is one full RK3 step (three stages of comp1 + comprhs +
-press + comp2) of the whole domain; metric = nx*ny*nz*steps / seconds.
+3/2-padded planes of 768x768), Re_tau=590, wall model isurface=6, seeded
+synthetic initial field (parabolic mean + uniform perturbations, projected
+divergence-free) built on the device, fixed dt at CFL 0.5.  A step is one
+full RK3 step (three stages of comp1 + comprhs + press + comp2) of the
+whole domain; metric = nx*ny*nz*steps / seconds.
 
-`value` is the plain FP64 drop-in form with the state resident in HBM;
-`forms` also reports the mixed form (FP32 transforms/advection/SGS, FP64
-pressure, mean modes and reductions).  `e2e` is the same metric through the
-C ABI a host program uses: the initial state is uploaded from pinned host
-memory inside the timed region and every step ends with les_gpu_stats
-(statistics read back to the host).
+Three forms run the same steps from the same initial field:
+  fp64          plain FP64 drop-in, Deardorff TKE closure;
+  mixed         FP32 transforms/advection/SGS, FP64 pressure, mean modes and
+                reductions, Deardorff closure;
+  learned_mixed the mixed form with the learned closure (bf16 network on
+                the tensor cores, weights from paes-channelflow_b200/weights,
+                Deardorff fallback when its mean dissipation is negative).
+`value` is learned_mixed (the metric compares it with fp64: `forms`), with
+the state resident in HBM; `errors` states its mean-profile, Reynolds-stress,
+rms and divergence differences from the fp64 run after the timed steps.
+`e2e` is the learned_mixed metric through the C ABI a host program uses:
+the state is uploaded from pinned host memory inside the timed region and
+every step ends with les_gpu_stats (statistics read back to the host).
 
 --impl reference times the CPU restatement of the reference (oracle/, FP64,
 OpenMP on all host cores) on a 512x512x4 slab of the same grid (the cost
@@ -123,6 +130,14 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def bf16_peak_tflops():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops_sustained"])
+    except Exception:
+        return 1400.0
+
+
 def algorithmic_bytes(kernel, nx, ny, nz, tb):
     """Compulsory HBM bytes of one launch (one stage over all levels) of the
     stage kernels: every array the kernel must read once and write once."""
@@ -151,10 +166,28 @@ def algorithmic_bytes(kernel, nx, ny, nz, tb):
     return table.get(kernel)
 
 
-def run_form(P, precision, steps, warmup, dev, want_profile):
+WEIGHTS = os.path.join(ROOT, "paes-channelflow_b200", "weights", "sgs_c4.npz")
+
+
+def load_network(P, dev):
+    """The trained closure (weights file), else a seeded untrained network."""
+    if os.path.exists(WEIGHTS):
+        z = np.load(WEIGHTS)
+        return P.Mlp(z["params"], z["norm"], device=dev), "trained (%s)" % os.path.relpath(WEIGHTS, ROOT)
+    rng = np.random.default_rng(0)
+    shapes = [(64, 11), (64,), (64, 64), (64,), (64, 64), (64,), (6, 64), (6,)]
+    p = np.concatenate([rng.standard_normal(sh).ravel() / np.sqrt(sh[-1]) if len(sh) == 2 else np.zeros(sh)
+                        for sh in shapes]).astype(np.float32)
+    norm = np.concatenate([np.zeros(11), np.full(9, 30.0), [1.0 / RE_TAU, 0.0], np.full(6, 1e-3), np.zeros(6)])
+    return P.Mlp(p, norm, device=dev), "untrained (seeded)"
+
+
+def run_form(P, precision, steps, warmup, dev, want_profile, imodel=3, mlp=None):
     import torch
-    cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=precision, device=dev)
+    cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=precision, device=dev, imodel=imodel)
     g = P.LesGpu(cfg)
+    if mlp is not None:
+        g.set_mlp(mlp, RE_TAU)
     g.make_ic(seed=12345, amp=0.1, re_tau=RE_TAU)
     dt = g.cfl_dt(0.5)
     g.cfg.dt = dt
@@ -183,16 +216,21 @@ def run_form(P, precision, steps, warmup, dev, want_profile):
     mb, sc = g.stats()
     out["utau"] = float(sc[0])
     out["divz_max"] = float(np.max(mb[2]))
+    out["meanbuf"] = mb
+    if mlp is not None:
+        out["learned_status"] = g.learned_status()
     out["handle"] = g
     return out
 
 
-def run_e2e(P, steps, dev):
+def run_e2e(P, steps, dev, precision, imodel=3, mlp=None):
     """Through the C ABI with host buffers: upload the state from pinned host
     memory, then steps x (les_gpu_step + les_gpu_stats read-back)."""
     import torch
-    cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=P.PREC_FP64, device=dev)
+    cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=precision, device=dev, imodel=imodel)
     g = P.LesGpu(cfg)
+    if mlp is not None:
+        g.set_mlp(mlp, RE_TAU)
     g.make_ic(seed=12345, amp=0.1, re_tau=RE_TAU)
     dt = g.cfl_dt(0.5)
     shape = (NZ, NY, NX)
@@ -297,21 +335,40 @@ def main():
     P = load_product()
 
     r64 = run_form(P, P.PREC_FP64, args.steps, args.warmup, dev, want_profile=True)
-    prof = r64.pop("profile")
+    prof64 = r64.pop("profile")
     r64.pop("handle").close()
     r32 = run_form(P, P.PREC_MIXED, args.steps, args.warmup, dev, want_profile=True)
     prof32 = r32.pop("profile")
     r32.pop("handle").close()
     torch.cuda.empty_cache()
-    e2e_s, h2d, d2h = run_e2e(P, args.steps, dev)
+    mlp, weights = load_network(P, dev)
+    rl = run_form(P, P.PREC_MIXED, args.steps, args.warmup, dev, want_profile=True, imodel=P.SGS_LEARNED, mlp=mlp)
+    prof = rl.pop("profile")
+    rl.pop("handle").close()
+    torch.cuda.empty_cache()
+    e2e_s, h2d, d2h = run_e2e(P, args.steps, dev, P.PREC_MIXED, imodel=P.SGS_LEARNED, mlp=mlp)
+    mlp.close()
 
     pts = NX * NY * NZ
     ms64 = max_over_ranks(r64["ms"])
     ms32 = max_over_ranks(r32["ms"])
+    msl = max_over_ranks(rl["ms"])
     e2e_s = max_over_ranks(e2e_s)
-    value = world * pts * args.steps / (ms64 / 1e3) / 1e6
+    fp64 = world * pts * args.steps / (ms64 / 1e3) / 1e6
     mixed = world * pts * args.steps / (ms32 / 1e3) / 1e6
+    value = world * pts * args.steps / (msl / 1e3) / 1e6
     e2e = world * pts * args.steps / e2e_s / 1e6
+
+    # stated errors of the learned mixed (and mixed Deardorff) form against fp64
+    def errors(r):
+        a, b = r["meanbuf"], r64["meanbuf"]
+        ub = float(np.mean(b[3]))
+        rms = lambda m: np.sqrt(np.maximum(m[6], 0))
+        return {"mean_u_max_err_over_ub": float(np.abs(a[3] - b[3]).max() / ub),
+                "uw_max_err_over_max": float(np.abs(a[9] - b[9]).max() / max(np.abs(b[9]).max(), 1e-300)),
+                "u_rms_max_err_over_max": float(np.abs(rms(a) - rms(b)).max() / max(rms(b).max(), 1e-300)),
+                "divz_max": float(np.max(a[2])), "divz_max_fp64": float(np.max(b[2])),
+                "after_steps": args.warmup + args.steps}
 
     # roofline of the dominant kernel (per-kernel CUDA events on the handle's stream)
     agg = {}
@@ -322,7 +379,7 @@ def main():
     top = max(agg.items(), key=lambda kv: kv[1][1])
     kname, (kfull, kms) = top[0], top[1]
     peak, peak_kind = peaks()
-    ab = algorithmic_bytes(kname, NX, NY, NZ, 8)
+    ab = algorithmic_bytes(kname, NX, NY, NZ, 4)
     achieved = ab / (kms / 1e3) / 1e9 if ab else None
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic_c5.txt")
@@ -332,27 +389,43 @@ def main():
             if len(f) >= 3 and f[0] == kname:
                 traffic = float(f[2])
     stage_ms = sum(t for _, t in prof)
+    # the network's tensor-core kernel: 2*(11*64 + 2*64*64 + 64*6) flops per point
+    fpp = 2 * (11 * 64 + 2 * 64 * 64 + 64 * 6)
+    mlp_ms = sum(t for n, t in prof if n.startswith("k_mlp_infer"))
+    mlp_tf = (fpp * pts / (mlp_ms / 1e3) / 1e12) if mlp_ms else None
+    bf16_peak = bf16_peak_tflops()
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mpoint-steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "channel 512x512x256 (3/2-padded 768x768), Re_tau=590, Deardorff TKE, isurface=6, "
-                               "RK3 at CFL 0.5, seeded projected random IC",
+        "warmup": args.warmup, "ms_per_step": msl / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "mixed: f32 transforms/advection/SGS, bf16 network, f64 pressure/reductions",
+        "data": "synthetic",
+        "config": {"workload": "channel 512x512x256 (3/2-padded 768x768), Re_tau=590, learned SGS closure with "
+                               "Deardorff fallback, mixed precision, isurface=6, RK3 at CFL 0.5, seeded projected "
+                               "random IC", "network": weights,
                    "global_batch": pts * world, "seq_len": None, "parallelism": "replicas%d" % world,
                    "l2": "working set (tens of GB) >> 126 MB L2; no flush needed"},
-        "forms": {"fp64": value, "mixed": mixed, "mixed_vs_fp64": mixed / value,
-                  "fp64_ms_per_step": ms64 / args.steps, "mixed_ms_per_step": ms32 / args.steps},
+        "forms": {"learned_mixed": value, "fp64": fp64, "mixed": mixed,
+                  "learned_mixed_vs_fp64": value / fp64, "mixed_vs_fp64": mixed / fp64,
+                  "fp64_ms_per_step": ms64 / args.steps, "mixed_ms_per_step": ms32 / args.steps,
+                  "learned_mixed_ms_per_step": msl / args.steps,
+                  "learned_used_last_stage": rl["learned_status"][0],
+                  "learned_dissipation_last_stage": rl["learned_status"][1]},
+        "errors": {"learned_mixed_vs_fp64": errors(rl), "mixed_vs_fp64": errors(r32)},
         "e2e": {"value": e2e, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": r64["launches"],
-        "clocks": r64["clocks"],
+        "gpu_launches": rl["launches"],
+        "clocks": rl["clocks"],
         "roofline": {"bound": "hbm", "kernel": kfull, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind, "kernel_ms": kms, "stage_ms": stage_ms,
                      "algorithmic_bytes": ab},
-        "kernels_ms_stage2": {n: round(t, 4) for n, t in prof},
+        "roofline_network": {"bound": "tensor", "kernel": "k_mlp_infer", "achieved": mlp_tf, "peak": bf16_peak,
+                             "unit": "TFLOP/s", "frac": (mlp_tf / bf16_peak) if mlp_tf else None,
+                             "kernel_ms": mlp_ms, "flops_per_point": fpp, "peak_source": "measured sustained"},
+        "kernels_ms_stage2_learned_mixed": {n: round(t, 4) for n, t in prof},
+        "kernels_ms_stage2_fp64": {n: round(t, 4) for n, t in prof64},
         "kernels_ms_stage2_mixed": {n: round(t, 4) for n, t in prof32},
-        "physics": {"utau": r64["utau"], "divz_max": r64["divz_max"], "dt": r64["dt"]},
+        "physics": {"utau": rl["utau"], "divz_max": rl["divz_max"], "dt": rl["dt"]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, el = cpu_baseline(1)

@@ -87,13 +87,16 @@ int les_gpu_learned_status(les_handle* h, int* used, double* dissipation);
  * cell size and truncation to the coarse modes in x and y.  out: 9 planes
  * of (nnz/fz, nny/fxy, nnx/fxy) doubles, in order u, v (cell centres),
  * w (coarse w-levels), tau11, tau22, tau33, tau12, tau13, tau23 with
- * tau_ij = filt(u_i u_j) - filt(u_i) filt(u_j) (w averaged to the centres).
+ * tau_ij = filt(u_i u_j) - filt(u_i) filt(u_j) (w averaged to the centres);
+ * with_model != 0 adds the filtered Deardorff stress of the fine run,
+ * -2 nu_t S_ij with nu_t = 0.1 dsl sqrt(e) at the fine cell centres, so
+ * tau_ij is the total sub-filter stress the coarse grid misses.
  *
  * les_gpu_learned_features: the network's raw inputs at every cell centre
  * of the current state, f32 [nnx*nny*nnz][16] (columns 0..10 as in the
  * feature list above, unnormalised; 11..15 zero), computed by the kernels
  * the learned stage uses. */
-int les_gpu_learn_filter(les_handle* h, int fxy, int fz, double* out);
+int les_gpu_learn_filter(les_handle* h, int fxy, int fz, int with_model, double* out);
 int les_gpu_learned_features(les_handle* h, double re_tau, float* feat);
 
 #ifdef __cplusplus

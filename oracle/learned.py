@@ -148,13 +148,35 @@ def _filter_xy(q, nxc, nyc, xl, yl):
     return np.fft.irfft2(C * (nxc * nyc), s=(nyc, nxc))
 
 
-def filter_fields(u, v, w, xl, yl, fxy, fz):
+def model_stress(u, v, w, e, xl, yl, zl, emin=1e-6):
+    """The fine run's Deardorff stress -2 nu_t S_ij at the cell centres,
+    nu_t = 0.1 dsl sqrt(max(e_c, emin)), e_c the mean of the cell's two
+    faces (e holds faces 1..nz at levels 1..nz; faces 0 and nz take the
+    values of faces 1 and nz-1).  Order tau11, tau22, tau33, tau12, tau13,
+    tau23."""
+    nz, ny, nx = u.shape
+    dz = zl / nz
+    dsl = (xl / nx * yl / ny * dz) ** (1.0 / 3.0)
+    g = gradients(u, v, w, xl, yl, zl)
+    face = lambda k: e[min(max(k, 1), nz - 1) - 1]
+    ec = np.stack([0.5 * (face(k) + face(k - 1)) for k in range(1, nz + 1)])
+    nu2 = 0.2 * dsl * np.sqrt(np.maximum(ec, emin))
+    return np.stack([-nu2 * g[0], -nu2 * g[4], -nu2 * g[8], -nu2 * 0.5 * (g[3] + g[1]),
+                     -nu2 * 0.5 * (g[6] + g[2]), -nu2 * 0.5 * (g[7] + g[5])])
+
+
+def filter_fields(u, v, w, xl, yl, fxy, fz, tau_model=None):
     """(9, nz/fz, ny/fxy, nx/fxy): u, v, w (coarse w-levels), tau11, tau22,
-    tau33, tau12, tau13, tau23."""
+    tau33, tau12, tau13, tau23; with tau_model (the fine run's own stress at
+    the cell centres, model_stress()) the stresses are the filtered total
+    sub-filter stress."""
     nz, ny, nx = u.shape
     nzc, nyc, nxc = nz // fz, ny // fxy, nx // fxy
     wc = np.stack([0.5 * (_wl(w, k, nz) + _wl(w, k - 1, nz)) for k in range(1, nz + 1)])
     q = [u, v, wc, u * u, v * v, wc * wc, u * v, u * wc, v * wc]
+    if tau_model is not None:
+        for i in range(6):
+            q[3 + i] = q[3 + i] + tau_model[i]
     qz = [a.reshape(nzc, fz, ny, nx).mean(axis=1) for a in q]
     if fz == 2:
         wst = np.stack([0.25 * _wl(w, 2 * K - 1, nz) + 0.5 * _wl(w, 2 * K, nz) + 0.25 * _wl(w, 2 * K + 1, nz)

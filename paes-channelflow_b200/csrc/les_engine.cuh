@@ -149,7 +149,7 @@ struct EngineBase {
   virtual void set_mlp(const MlpDev* p, double re_tau) = 0;
   virtual void learned_status(int* used, double* dissipation) = 0;
   virtual void learned_features(double re_tau, float* feat) = 0;
-  virtual void learn_filter(int fxy, int fz, double* out) = 0;
+  virtual void learn_filter(int fxy, int fz, int with_model, double* out) = 0;
 };
 
 template <class T>
@@ -517,7 +517,7 @@ struct Engine : EngineBase {
            (long long)ps, (T)dsl, (T)dz, (T)cfg.zl, (T)(rt / (cfg.zl / 2.0)));
   }
   // explicit filter of the current state onto the grid (NX/fxy, NY/fxy, NZ/fz)
-  void learn_filter(int fxy, int fz, double* out) override {
+  void learn_filter(int fxy, int fz, int with_model, double* out) override {
     if (phase != 0) throw std::logic_error("learn_filter inside a split comp1..comp2 sequence");
     if (fxy < 1 || fz < 1 || fz > 2 || NX % fxy || NY % fxy || NZ % fz)
       throw std::invalid_argument("learn_filter: unsupported filter factors for this grid");
@@ -529,11 +529,16 @@ struct Engine : EngineBase {
     if (fsh.n < npl * nm) { fsh.release(); fsh.alloc(npl * nm); }
     if (fch.n < npl * nmc) { fch.release(); fch.alloc(npl * nmc); }
     if (fcp.n < npl * psc) { fcp.release(); fcp.alloc(npl * psc); }
+    if (with_model) {
+      learned_alloc();
+      learned_gradients();
+    }
     to_physical(uh.p, phys[0].p, NZ);
     to_physical(vh.p, phys[1].p, NZ);
     to_physical(wh.p, phys[2].p, NZ);
     launch(k_filt_z<T>, dim3(cdiv(ps, 256), NZc), dim3(256), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
-           (const T*)phys[2].p, fscr.p, (long long)ps, NZ, NZc, fz);
+           (const T*)phys[2].p, with_model ? (const T*)lphys.p : (const T*)nullptr, (const T*)e.p, (T)dsl,
+           (T)cfg.emin, fscr.p, (long long)ps, NZ, NZc, fz);
     with_small(NX, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = RowCfg<NN>;

@@ -162,11 +162,12 @@ template <int N> __device__ __forceinline__ int stockham_twiddle_exp(int i) {
   return k * r * (N / (R1 * R2 * R3));
 }
 
-// Transform used by the fused kernel for a (length, type): the two-pass
-// warp form unless its N2-point register DFT would not fit (FP64 at 768),
-// then the three-pass Stockham form.
+// Transform used by the fused kernel for a length: the two-pass warp form
+// unless its N2-point register DFT is longer than 24 (768 = 24 x 32), then
+// the three-pass Stockham form (radices <= 12, no register spills in either
+// precision).
 template <int N, class T> struct FusedPlan {
-  static constexpr bool three = (sizeof(T) == 8 && Split<N>::N2 > 24);
+  static constexpr bool three = (Split<N>::N2 > 24);
   static constexpr int BUF = three ? N : smem_fft_elems<N, false>(1);
 };
 template <int N, int S, bool IN_SMEM, class T, class LoadF>

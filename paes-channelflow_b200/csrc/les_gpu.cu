@@ -475,10 +475,10 @@ extern "C" int les_gpu_learned_status(les_handle* h, int* used, double* dissipat
   return guarded(h, [&] { h->eng->learned_status(used, dissipation); });
 }
 
-extern "C" int les_gpu_learn_filter(les_handle* h, int fxy, int fz, double* out) {
+extern "C" int les_gpu_learn_filter(les_handle* h, int fxy, int fz, int with_model, double* out) {
   if (!h || !out) return LES_EINVAL;
   return guarded(h, [&] {
-    h->eng->learn_filter(fxy, fz, out);
+    h->eng->learn_filter(fxy, fz, with_model, out);
     LES_CUDA(cudaStreamSynchronize(h->eng->stream()));
   });
 }

@@ -185,13 +185,25 @@ namespace les {
 // the fine centres), and w at the coarse w-levels (fz = 2: weights 1/4,
 // 1/2, 1/4 of the fine w-levels 2K-1, 2K, 2K+1).
 // ---------------------------------------------------------------------------
+// With G (the fine run's nine gradient planes at the cell centres, [9][NZ][ps])
+// and E (its TKE at the w-levels, plane k = level k), the fine run's own
+// Deardorff stress -2 nu_t S_ij, nu_t = 0.1 dsl sqrt(max(e_c, emin)) with e_c
+// the average of the two faces of the cell (faces 0 and nnz take the values
+// of faces 1 and nnz-1), is added to the products before filtering, so the
+// stresses come out as the filtered total sub-filter stress.
 template <class T>
 __global__ void k_filt_z(const T* __restrict__ U, const T* __restrict__ V, const T* __restrict__ W,
-                         T* __restrict__ S, long long ps, int NZ, int NZc, int fz) {
+                         const T* __restrict__ G, const T* __restrict__ E, T dsl, T emin, T* __restrict__ S,
+                         long long ps, int NZ, int NZc, int fz) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int K = blockIdx.y + 1;
   if (p >= ps) return;
   auto w = [&](int k) -> T { return (k >= 1 && k <= NZ - 1) ? W[(size_t)(k - 1) * ps + p] : (T)0; };
+  auto ef = [&](int k) -> T {
+    k = k < 1 ? 1 : (k > NZ - 1 ? NZ - 1 : k);
+    return E[(size_t)k * ps + p];
+  };
+  const size_t N = (size_t)NZ * ps;
   T q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int j = 0; j < fz; j++) {
     const int k = fz * (K - 1) + 1 + j;
@@ -200,6 +212,21 @@ __global__ void k_filt_z(const T* __restrict__ U, const T* __restrict__ V, const
     q[0] += u; q[1] += v; q[2] += wc;
     q[3] += u * u; q[4] += v * v; q[5] += wc * wc;
     q[6] += u * v; q[7] += u * wc; q[8] += v * wc;
+    if (G) {
+      const size_t o = (size_t)(k - 1) * ps + p;
+      T g[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) g[i] = G[i * N + o];  // ux, vx, wx, uy, vy, wy, uz, vz, wz
+      T ec = (T)0.5 * (ef(k) + ef(k - 1));
+      ec = ec > emin ? ec : emin;
+      const T nu2 = (T)0.2 * dsl * sqrt(ec);
+      q[3] -= nu2 * g[0];
+      q[4] -= nu2 * g[4];
+      q[5] -= nu2 * g[8];
+      q[6] -= nu2 * (T)0.5 * (g[3] + g[1]);
+      q[7] -= nu2 * (T)0.5 * (g[6] + g[2]);
+      q[8] -= nu2 * (T)0.5 * (g[7] + g[5]);
+    }
   }
   const T inv = (T)1 / (T)fz;
   const size_t plane = (size_t)NZc * ps;

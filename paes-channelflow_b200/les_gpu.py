@@ -132,7 +132,7 @@ def lib():
         "les_mlp_adam_step": (I, [VP, VP, VP, ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(D), VP]),
         "les_gpu_set_mlp": (I, [H, VP, D]),
         "les_gpu_learned_status": (I, [H, ctypes.POINTER(I), ctypes.POINTER(D)]),
-        "les_gpu_learn_filter": (I, [H, I, I, VP]),
+        "les_gpu_learn_filter": (I, [H, I, I, I, VP]),
         "les_gpu_learned_features": (I, [H, D, VP]),
     }
     for name, (res, args) in sig.items():
@@ -286,15 +286,16 @@ class LesGpu:
         self._check(lib().les_gpu_learned_status(self.h, ctypes.byref(used), ctypes.byref(d)))
         return used.value, d.value
 
-    def learn_filter(self, fxy, fz):
+    def learn_filter(self, fxy, fz, with_model=True):
         """Filtered coarse fields of the current state: float64 CUDA tensor
         (9, nnz/fz, nny/fxy, nnx/fxy) = u, v, w, tau11, tau22, tau33, tau12,
-        tau13, tau23."""
+        tau13, tau23 (with_model: tau includes the filtered Deardorff stress
+        of this run)."""
         import torch
         c = self.cfg
         out = torch.empty((9, c.nnz // fz, c.nny // fxy, c.nnx // fxy), dtype=torch.float64,
                           device="cuda:%d" % c.device)
-        self._check(lib().les_gpu_learn_filter(self.h, fxy, fz, out.data_ptr()))
+        self._check(lib().les_gpu_learn_filter(self.h, fxy, fz, int(with_model), out.data_ptr()))
         return out
 
     def learned_features(self, re_tau):

@@ -11,7 +11,11 @@
    an FP64 handle for the data.
 2. After the spin-up, every `every` steps: les_gpu_learn_filter onto the
    coarse grid (box filter: `fxy` fine cells in x, y and `fz` in z) gives
-   the filtered u, v, w and tau_ij = filt(u_i u_j) - filt(u_i) filt(u_j);
+   the filtered u, v, w and tau_ij = filt(u_i u_j) - filt(u_i) filt(u_j)
+   plus (by default) the filtered Deardorff stress of the fine run itself,
+   i.e. the total sub-filter stress the coarse grid misses (without it the
+   targets lack the momentum flux the fine run's model carries near the
+   walls, and coarse runs with the network lose their near-wall velocity);
    the filtered fields are loaded into a coarse handle whose
    les_gpu_learned_features computes the network inputs with the same
    kernels the learned stage uses.
@@ -82,7 +86,7 @@ def loglaw_field(cfg, amp, seed, large=0.0, utau=float(np.sqrt(0.016)), kappa=0.
 
 
 def collect(fine=(384, 384, 192), factor=(4, 2), re_tau=395.0, snapshots=200, spinup=14000, every=40, amp=1.0,
-            large=0.3, seed=12345, cfl=0.5, spinup_precision=4, log=print):
+            large=0.3, seed=12345, cfl=0.5, spinup_precision=4, with_model=True, log=print):
     """Run the fine case and return (features f32 (S, Nc, 16), targets f64
     (S, Nc, 6), info, first filtered (u, v, w)) with the sample arrays as
     CUDA tensors."""
@@ -135,7 +139,7 @@ def collect(fine=(384, 384, 192), factor=(4, 2), re_tau=395.0, snapshots=200, sp
             for _ in range(every):
                 g.step(it=state["it"], mnout=False, dt=dt)
                 state["it"] += 1
-        out = g.learn_filter(fxy, fz)
+        out = g.learn_filter(fxy, fz, with_model=with_model)
         uvw = out[:3].cpu().numpy()
         if first is None:
             first = uvw.copy()
@@ -148,6 +152,7 @@ def collect(fine=(384, 384, 192), factor=(4, 2), re_tau=395.0, snapshots=200, sp
     g.sync()
     info = dict(fine=list(fine), factor=list(factor), re_tau=re_tau, snapshots=snapshots, spinup=spinup,
                 spinup_precision=spinup_precision, every=every, amp=amp, large=large, seed=seed, dt=dt,
+                targets="filtered total sub-filter stress" if with_model else "filtered minus resolved products",
                 steps=state["it"], coarse=[nx // fxy, ny // fxy, nz // fz], history=hist,
                 collect_seconds=time.time() - t0, filtered_mean_u=np.mean(fine_means, axis=0).tolist(), z0=cfg.z0)
     g.close()
@@ -312,7 +317,8 @@ def run(args, log=print):
     t_all = time.time()
     feats, targs, info, first = collect(tuple(args.fine), tuple(args.factor), args.re_tau, args.snapshots,
                                         args.spinup, args.every, args.amp, args.large, args.seed,
-                                        spinup_precision=args.spinup_precision, log=log)
+                                        spinup_precision=args.spinup_precision,
+                                        with_model=not getattr(args, "resolved_only", False), log=log)
     S = feats.shape[0]
     nho = max(1, int(round(S * args.holdout)))
     ftr, ttr = feats[:S - nho], targs[:S - nho]
@@ -362,6 +368,8 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--aposteriori", type=int, default=0, help="coarse steps of the a-posteriori runs (0 = skip)")
+    ap.add_argument("--resolved-only", action="store_true",
+                    help="targets without the fine run's own model stress")
     ap.add_argument("--out", default=os.path.join(HERE, "weights", "sgs_c4"))
     args = ap.parse_args(argv)
     run(args)

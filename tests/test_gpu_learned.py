@@ -104,11 +104,16 @@ def test_set_mlp_rejects_other_closures(gpu_lib, product):
     assert ei.value.code == product.LES_EINVAL
 
 
-def test_learn_filter_matches_numpy(gpu_lib, product):
+@pytest.mark.parametrize("with_model", [False, True])
+def test_learn_filter_matches_numpy(gpu_lib, product, with_model):
     from oracle import learned as LN
     o, g, f = make_pair(product, 64, 64, 16, imodel=3)
-    out = g.learn_filter(4, 2).cpu().numpy()
-    ref = LN.filter_fields(f["u"], f["v"], f["w"], o.cfg.xl, o.cfg.yl, 4, 2)
+    c = o.cfg
+    e = 1e-3 * (1.0 + 0.5 * LN.Spec(64, 64, c.xl, c.yl).deal(np.random.default_rng(5).uniform(-1, 1, f["u"].shape)))
+    g.upload(f["u"], f["v"], f["w"], e, f["p"])
+    out = g.learn_filter(4, 2, with_model=with_model).cpu().numpy()
+    tm = LN.model_stress(f["u"], f["v"], f["w"], e, c.xl, c.yl, c.zl, c.emin) if with_model else None
+    ref = LN.filter_fields(f["u"], f["v"], f["w"], c.xl, c.yl, 4, 2, tau_model=tm)
     assert out.shape == ref.shape == (9, 8, 16, 16)
     us = np.abs(f["u"]).max()
     for i in range(9):
