@@ -115,7 +115,9 @@ def divergence(tau, xl, yl, zl):
     _, nz, ny, nx = tau.shape
     sp = Spec(nx, ny, xl, yl)
     dz = zl / nz
-    tw = lambda f, k: 0.5 * (tau[f, k - 1] + tau[f, k]) if 1 <= k <= nz - 1 else np.zeros((ny, nx))
+    # tau13, tau23 on the w-levels 2..nz-2; the walls and the wall-adjacent
+    # w-levels 1 and nz-1 keep the wall model's and the Deardorff stresses
+    tw = lambda f, k: 0.5 * (tau[f, k - 1] + tau[f, k]) if 2 <= k <= nz - 2 else np.zeros((ny, nx))
     lru = np.zeros((nz, ny, nx)); lrv = np.zeros_like(lru); lrw = np.zeros_like(lru)
     for k in range(1, nz + 1):
         t = lambda f: tau[f, k - 1]

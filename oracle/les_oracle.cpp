@@ -679,6 +679,8 @@ struct Les {
   void compsgs1(int iz, int j, int jp1, int k, int km1, int l, int lm1, int lp1, int nm1, int n, int np1,
                 int np2) {
     const T mom = sgs_mom;
+    // the wall-adjacent w-levels 1 and nnz-1 keep their shear stresses
+    const T momw = (iz == 1 || iz == nnz - 1) ? (T)1 : mom;
     if (iz == 1) {
       complen(lm1, -1, nm1, n);
       complen(l, 0, n, np1);
@@ -698,8 +700,8 @@ struct Les {
     } else {
       for (size_t i = 0; i < pb; i++) {
         tauww[jp1][i] = -mom * (XKK[l][i] + XKK[lp1][i]) * WZ[np1][i];
-        tauuw[k][i] = -mom * XKK[l][i] * (UZ[l][i] + WX[l][i]);
-        tauvw[k][i] = -mom * XKK[l][i] * (VZ[l][i] + WY[l][i]);
+        tauuw[k][i] = -momw * XKK[l][i] * (UZ[l][i] + WX[l][i]);
+        tauvw[k][i] = -momw * XKK[l][i] * (VZ[l][i] + WY[l][i]);
       }
     }
   }
@@ -761,8 +763,9 @@ struct Les {
   // stage uses the network when the mean of -tau_ij S_ij is >= 0, and then
   // adds the dealiased stress divergence to ru, rv, rw:
   //   ru += -d/dx tau11 - d/dy tau12 - (tau13w(k) - tau13w(k-1))/dz, ...
-  // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on interior w-levels and 0 on
-  // the walls (the wall model's stresses stay in compsgs1).
+  // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on the w-levels 2..nnz-2 and 0
+  // on the walls and the wall-adjacent w-levels 1 and nnz-1 (the wall model's
+  // and the Deardorff shear stresses stay there in compsgs1).
   void learned_prepare() {
     const int NZ = nnz;
     std::vector<std::vector<T>> tau((size_t)6 * (NZ + 2), std::vector<T>(ps, (T)0));
@@ -817,7 +820,7 @@ struct Les {
     // stress divergence
     std::vector<T> t13w_m(ps), t13w_p(ps), t23w_m(ps), t23w_p(ps), f1(ps), f2(ps);
     auto tw = [&](int f, int k, std::vector<T>& o) {
-      if (k < 1 || k > NZ - 1) { std::fill(o.begin(), o.end(), (T)0); return; }
+      if (k < 2 || k > NZ - 2) { std::fill(o.begin(), o.end(), (T)0); return; }
       for (size_t q = 0; q < ps; q++) o[q] = (T)0.5 * (TA(f, k)[q] + TA(f, k + 1)[q]);
     };
     for (int iz = 1; iz <= NZ; iz++) {

@@ -187,9 +187,9 @@ struct Engine : EngineBase {
   const MlpDev* mlp = nullptr;
   double re_tau = 0.0;
   int nsm = 148;
-  DevBuf<cx<T>> lgy;   // [9][NZ][NY][KX] gradient spectra along x; reused for tau^ [6][...]
-  DevBuf<T> lphys;     // [9][NZ][NY][NX] gradient planes; reused for tau [6][...]
-  DevBuf<uint4> lfeat; // [N][16] bf16 features
+  DevBuf<cx<T>> lgy;   // [9][NZ][NY][KX] gradient spectra along x
+  DevBuf<T> lphys;     // [9][NZ][NY][NX] gradient planes (features, filter); in the stage the
+                       // tau rows th [6][NZ][NY][KX] complex
   DevBuf<double> lpart, lstat;
   DevBuf<int> lflag;
   DevBuf<T> fscr, fcp;      // filter scratch: z-averaged fine planes, coarse planes
@@ -253,7 +253,7 @@ struct Engine : EngineBase {
     clipflag.release(); ephys.release(); dEX.release(); dEY.release(); wallpl.release();
     for (auto& b : xout) b.release();
     for (auto& b : phys) b.release();
-    lgy.release(); lphys.release(); lfeat.release(); lpart.release(); lstat.release(); lflag.release();
+    lgy.release(); lphys.release(); lpart.release(); lstat.release(); lflag.release();
     fscr.release(); fcp.release(); fsh.release(); fch.release();
   }
   cudaStream_t stream() override { return st; }
@@ -468,7 +468,6 @@ struct Engine : EngineBase {
     if (lgy.p) return;
     lgy.alloc(9 * nm * NZ);
     lphys.alloc(9 * ps * NZ);
-    lfeat.alloc(2 * ps * NZ);
     lpart.alloc(nsm);
     lstat.alloc(2);
     lflag.alloc(1);
@@ -570,34 +569,36 @@ struct Engine : EngineBase {
   // gradients -> features -> network -> tau and the fallback flag
   void learned_pre() {
     const size_t N = ps * NZ;
-    learned_gradients();
+    // gradient spectra along x at every level (lgy [9][NZ][NY][KX])
+    with_small(NY, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = ColCfg<NN, T>;
+      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC), NZ, 9), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
+             (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)kx0, (T)ky0, (T)dzm, tw);
+    });
+    // x transforms, features, network, tau rows (th = lphys storage as [6][NZ][NY][KX] complex)
     const double h = cfg.zl / 2.0;
-    launch(k_lfeat<T>, dim3(cdiv(N, 256)), dim3(256), 0, st, (const T*)lphys.p, lfeat.p, mlp, (long long)N,
-           (long long)ps, (T)dsl, (T)dz, (T)cfg.zl, (T)(re_tau / h));
-    const long long ntiles = ((long long)N + 127) / 128;
-    const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, nsm);
-    MlpOutTau<T> out{lphys.p, (long long)N};
-    launch(k_mlp_infer<MlpOutTau<T>>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, st, mlp,
-           (const uint4*)lfeat.p, (long long)N, out, lpart.p, err.p);
+    int grid = 1;
+    with_small(NX, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using L = LearnedRow<NN>;
+      grid = (int)std::min<size_t>(cdiv((size_t)NZ * NY, L::RB), (size_t)nsm);
+      launch(k_learned_row<T, NN>, dim3(grid), dim3(512), L::template smem<T>(), st, mlp, (const cx<T>*)lgy.p,
+             (cx<T>*)lphys.p, NY, NZ, (T)dsl, (T)dz, (T)cfg.zl, (T)(re_tau / h), tw, lpart.p, err.p);
+    });
     launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, 1.0 / ((double)N * dsl), lflag.p,
            lstat.p);
   }
   // tau^ and its divergence into the new tendencies
   void learned_post(const StageArgs& a) {
-    with_small(NX, [&](auto cn) {
-      constexpr int NN = decltype(cn)::value;
-      using C = RowCfg<NN>;
-      const size_t nrows = 6 * (size_t)NZ * NY;
-      launch(k_row_r2c<T, NN>, dim3(cdiv((nrows + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
-             (const T*)lphys.p, lgy.p, (int)nrows, KX, tw);
-    });
+    cx<T>* th = (cx<T>*)lphys.p;
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = ColCfg<NN, T>;
       launch(k_col_small<T, NN, false>, dim3(cdiv(KX, C::TC), 6 * NZ), dim3(C::THREADS), C::buf(), st,
-             (const cx<T>*)lgy.p, lgy.p, KX, (T)(1.0 / ((double)NX * NY)), tw);
+             (const cx<T>*)th, th, KX, (T)(1.0 / ((double)NX * NY)), tw);
     });
-    launch(k_ldiv<T>, dim3(cdiv(nm, 128), NZ), dim3(128), 0, st, (const cx<T>*)lgy.p, run.p, rvn.p, rwn.p,
+    launch(k_ldiv<T>, dim3(cdiv(nm, 128), NZ), dim3(128), 0, st, (const cx<T>*)th, run.p, rvn.p, rwn.p,
            (const int*)lflag.p, a);
   }
   // Wall-model plane sums from the physical U, V rows of levels 1 and nnz.

@@ -13,21 +13,25 @@
 //                 (the centred average of the w-level differences with
 //                  UZ(0) = UZ(1) and UZ(nnz) = UZ(nnz-1), as derivs1.f90 /
 //                  derivs2.f90 set the wall rows)
-//   2. k_row_c2r along x (shared with the rest of the stage);
-//   3. k_lfeat: normalised bf16 features;
-//   4. k_mlp_infer<MlpOutTau>: tau_ij on the tensor cores, and the per-CTA
-//      sums of the dissipation -tau_ij S_ij;
-//   5. k_learned_flag: plane-and-level mean of the dissipation (FP64, fixed
+//   2. k_learned_row: inverse x transforms, normalised bf16 features, the
+//      network on the tensor cores, tau_ij and the per-CTA sums of the
+//      dissipation -tau_ij S_ij, forward x transforms of tau (one kernel,
+//      nothing in between goes to HBM);
+//   3. k_learned_flag: plane-and-level mean of the dissipation (FP64, fixed
 //      order); flag = 1 when it is >= 0, else 0 (Deardorff fallback);
 //   ... the padded-grid kernels (their interior momentum stresses are
 //      multiplied by 1 - flag) ...
-//   6. k_row_r2c + k_col_small: tau^ at every level;
-//   7. k_ldiv: the stress divergence added to the new tendencies (when flag):
+//   4. k_col_small: y transforms of tau at every level;
+//   5. k_ldiv: the stress divergence added to the new tendencies (when flag):
 //        ru += -i kx tau11^ - i ky tau12^ - (tau13w^(k) - tau13w^(k-1)) / dz
 //        rv += -i kx tau12^ - i ky tau22^ - (tau23w^(k) - tau23w^(k-1)) / dz
 //        rw += -i kx tau13w^ - i ky tau23w^ - (tau33^(k+1) - tau33^(k)) / dz   (w-levels)
-//      with tau13w(k) = (tau13(k) + tau13(k+1)) / 2 on interior w-levels and 0
-//      on the walls (the wall model's stresses stay in the padded kernels).
+//      with tau13w(k) = (tau13(k) + tau13(k+1)) / 2 on the w-levels 2..nnz-2
+//      and 0 on the walls and the wall-adjacent w-levels 1 and nnz-1: there
+//      the padded kernels keep the wall model's and the Deardorff shear
+//      stresses (the network, trained on cell-centre stresses, under-predicts
+//      the flux through the first face, and coarse runs lose their near-wall
+//      velocity without this).
 // The kinetic-energy equation keeps the Deardorff eddy diffusivity.
 #pragma once
 #include "les_kernels.cuh"
@@ -79,55 +83,169 @@ k_lgrad_y(const cx<T>* __restrict__ uh, const cx<T>* __restrict__ vh, const cx<T
   });
 }
 
-// Normalised bf16 features [N][16] from the nine gradient planes [9][N].
-template <class T>
-__global__ void k_lfeat(const T* __restrict__ g, uint4* __restrict__ feat, const MlpDev* __restrict__ P, long long N,
-                        long long plane, T delta, T dz, T zl, T zplus_per_len) {
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= N) return;
-  const int z = (int)(p / plane);
-  const T zc = ((T)z + (T)0.5) * dz;
-  const T zw = zc < zl - zc ? zc : zl - zc;
-  float f[16];
-#pragma unroll
-  for (int j = 0; j < 9; j++) f[j] = (float)((g[(size_t)j * N + p] * delta - (T)P->in_shift[j]) * (T)P->in_scale[j]);
-  f[9] = (float)((zw * zplus_per_len - (T)P->in_shift[9]) * (T)P->in_scale[9]);
-  f[10] = (float)((delta - (T)P->in_shift[10]) * (T)P->in_scale[10]);
-#pragma unroll
-  for (int j = 11; j < 16; j++) f[j] = 0.f;
-  feat[2 * p] = make_uint4(pack_bf2(f[0], f[1]), pack_bf2(f[2], f[3]), pack_bf2(f[4], f[5]), pack_bf2(f[6], f[7]));
-  feat[2 * p + 1] = make_uint4(pack_bf2(f[8], f[9]), pack_bf2(f[10], 0.f), 0u, 0u);
-}
-
 __device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
 
-// Network outputs -> tau planes [6][N] (tau11, tau22, tau33, tau12, tau13,
-// tau23) and the dissipation -tau_ij S_ij * Delta from the features.
-template <class T> struct MlpOutTau {
-  T* tau;
-  long long N;
-  __device__ double operator()(long long p, bool valid, const float (&y)[16], uint4 f0, uint4 f1,
-                               const MlpDev* P) const {
-    if (!valid) return 0.0;
-    float t[6];
-#pragma unroll
-    for (int i = 0; i < 6; i++) {
-      t[i] = y[i] * P->out_scale[i] + P->out_shift[i];
-      tau[(size_t)i * N + p] = (T)t[i];
-    }
-    const float q[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
-                        bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
-    float g[9];
-#pragma unroll
-    for (int j = 0; j < 9; j++) g[j] = q[j] / P->in_scale[j] + P->in_shift[j];  // d_i u_j * Delta
-    // g = (ux, vx, wx, uy, vy, wy, uz, vz, wz) * Delta
-    const float s11 = g[0], s22 = g[4], s33 = g[8];
-    const float s12 = 0.5f * (g[3] + g[1]), s13 = 0.5f * (g[6] + g[2]), s23 = 0.5f * (g[7] + g[5]);
-    return -((double)t[0] * s11 + (double)t[1] * s22 + (double)t[2] * s33 +
-             2.0 * ((double)t[3] * s12 + (double)t[4] * s13 + (double)t[5] * s23));
+// ---------------------------------------------------------------------------
+// The learned stage's x-direction work in one persistent kernel per SM: for
+// a block of RB rows (one level z, consecutive y) of the gradient spectra
+// from k_lgrad_y it does
+//   1. the inverse x transforms of the nine gradient rows (five complex
+//      transforms per row, two real rows each, as k_row_c2r),
+//   2. the normalised bf16 features, one sample per thread (thread i =
+//      point i of the block = row i%128 of group i/128's tile),
+//   3. the network on the tensor cores (mlp_tile, four groups),
+//   4. tau_ij and the dissipation -tau_ij S_ij (as MlpOutTau),
+//   5. the forward x transforms of the six tau rows with the real-pair
+//      separation of k_row_r2c, written as x-spectral rows th[6][NZ][NY][KX]
+//      (kx < nx/2, unscaled) for the y transforms of k_col_small.
+// Nothing between steps 1 and 5 goes to HBM.
+// ---------------------------------------------------------------------------
+template <int NX> struct LearnedRow {
+  static constexpr int N1 = Split<NX>::N1, N2 = Split<NX>::N2, M12 = N1 > N2 ? N1 : N2;
+  static constexpr int RB0 = 512 / NX, RB1 = 512 / (5 * M12);
+  static constexpr int RB = (RB0 < RB1 ? RB0 : RB1) > 0 ? (RB0 < RB1 ? RB0 : RB1) : 1;  // rows per block
+  template <class T> static constexpr size_t fft_bytes() {
+    return (size_t)smem_fft_elems<NX, false>(5 * RB) * sizeof(cx<T>);
+  }
+  template <class T> static constexpr size_t smem() {
+    return sizeof(MlpDev) + (size_t)4 * 16384 + fft_bytes<T>() + 256;
   }
 };
+
+template <class T, int NX>
+__global__ void __launch_bounds__(512, 1)
+k_learned_row(const MlpDev* __restrict__ prm, const cx<T>* __restrict__ gy, cx<T>* __restrict__ th, int NY,
+              int NZ, T delta, T dz, T zl, T zplus_per_len, const cx<T>* __restrict__ tw,
+              double* __restrict__ dissip_part, int* __restrict__ err) {
+  using L = LearnedRow<NX>;
+  constexpr int KX = NX / 2, RB = L::RB, NTI = 5 * RB, NTF = 3 * RB;
+  extern __shared__ __align__(1024) unsigned char smraw_tc[];
+  MlpDev* P = reinterpret_cast<MlpDev*>(smraw_tc);
+  unsigned char* act_all = smraw_tc + sizeof(MlpDev);
+  cx<T>* fb = reinterpret_cast<cx<T>*>(act_all + 4 * 16384);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(act_all + 4 * 16384 + L::template fft_bytes<T>());
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 4);
+  double* red = reinterpret_cast<double*>(bars + 5);
+
+  const int tid = threadIdx.x, g = tid >> 7, r = tid & 127, warp = tid >> 5, q = warp & 3;
+  for (int i = tid; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
+    reinterpret_cast<uint4*>(P)[i] = reinterpret_cast<const uint4*>(prm)[i];
+  if (tid < 4) tc::mbar_init(&bars[tid], 1);
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, 256);
+    tc::tmem_relinquish();
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *tslot;
+  MlpGroup grp = mlp_group(P, act_all + (size_t)g * 16384, tbase, g, q, &bars[g]);
+
+  const size_t R = (size_t)NZ * NY;
+  const size_t plane = R * KX;
+  double dsum = 0.0;
+  bool failed = false;
+  for (size_t r0 = (size_t)blockIdx.x * RB; r0 < R; r0 += (size_t)gridDim.x * RB) {
+    // 1. inverse x transforms: transform t = 5*rr + j packs gradient rows 2j, 2j+1 of row r0+rr
+    fft_core<NX, +1, false, false, true>(NTI, fb, tw, [&](int t, int n) -> cx<T> {
+      const int rr = t / 5, j = t - 5 * rr;
+      const size_t row = r0 + rr;
+      if (row >= R) return zero_cx<T>();
+      int k = n;
+      bool mir = false;
+      if (k >= KX) {
+        if (NX - k < KX) { k = NX - k; mir = true; }
+        else k = -1;
+      }
+      if (k < 0) return zero_cx<T>();
+      cx<T> a = gy[(size_t)(2 * j) * plane + row * KX + k];
+      cx<T> b = (j < 4) ? gy[(size_t)(2 * j + 1) * plane + row * KX + k] : zero_cx<T>();
+      if (k == 0) { a.y = 0; b.y = 0; }
+      if (mir) { a = conj(a); b = conj(b); }
+      return mk(a.x - b.y, a.y + b.x);
+    }, NoStore{});
+    // 2. features of this thread's point
+    const int rr = tid / NX, x = tid - (tid / NX) * NX;
+    const size_t row = r0 + rr;
+    const bool valid = (tid < RB * NX) && (row < R);
+    uint4 f0 = make_uint4(0, 0, 0, 0), f1 = f0;
+    if (valid) {
+      T gv[9];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const cx<T> v = fb[(size_t)(5 * rr + j) * NX + x];
+        gv[2 * j] = v.x;
+        if (j < 4) gv[2 * j + 1] = v.y;
+      }
+      const int z = (int)(row / NY);
+      const T zc = ((T)z + (T)0.5) * dz;
+      const T zw = zc < zl - zc ? zc : zl - zc;
+      float f[11];
+#pragma unroll
+      for (int j = 0; j < 9; j++) f[j] = (float)((gv[j] * delta - (T)P->in_shift[j]) * (T)P->in_scale[j]);
+      f[9] = (float)((zw * zplus_per_len - (T)P->in_shift[9]) * (T)P->in_scale[9]);
+      f[10] = (float)((delta - (T)P->in_shift[10]) * (T)P->in_scale[10]);
+      f0 = make_uint4(pack_bf2(f[0], f[1]), pack_bf2(f[2], f[3]), pack_bf2(f[4], f[5]), pack_bf2(f[6], f[7]));
+      f1 = make_uint4(pack_bf2(f[8], f[9]), pack_bf2(f[10], 0.f), 0u, 0u);
+    }
+    __syncthreads();  // every gradient read from fb before tau is written there
+    // 3. the network
+    float y[16];
+    const bool ok = mlp_tile(grp, P, r, f0, f1, y);
+    if (!ok) mlp_tile_failed(grp, r, err);
+    // 4. tau into the forward transform rows: (tau11, tau12), (tau22, tau33), (tau13, tau23)
+    if (valid && ok) {
+      float t[6];
+#pragma unroll
+      for (int i = 0; i < 6; i++) t[i] = y[i] * P->out_scale[i] + P->out_shift[i];
+      fb[(size_t)(3 * rr + 0) * NX + x] = mk((T)t[0], (T)t[3]);
+      fb[(size_t)(3 * rr + 1) * NX + x] = mk((T)t[1], (T)t[2]);
+      fb[(size_t)(3 * rr + 2) * NX + x] = mk((T)t[4], (T)t[5]);
+      const float qv[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
+                           bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
+      float gg[9];
+#pragma unroll
+      for (int j = 0; j < 9; j++) gg[j] = qv[j] / P->in_scale[j] + P->in_shift[j];
+      const float s11 = gg[0], s22 = gg[4], s33 = gg[8];
+      const float s12 = 0.5f * (gg[3] + gg[1]), s13 = 0.5f * (gg[6] + gg[2]), s23 = 0.5f * (gg[7] + gg[5]);
+      dsum -= (double)t[0] * s11 + (double)t[1] * s22 + (double)t[2] * s33 +
+              2.0 * ((double)t[3] * s12 + (double)t[4] * s13 + (double)t[5] * s23);
+    }
+    if (__syncthreads_or(!ok)) { failed = true; break; }
+    // 5. forward x transforms and the real-pair separation
+    fft_core<NX, -1, false, true, true>(NTF, fb, tw, NoLoad{}, NoStore{});
+    for (int i = tid; i < NTF * KX; i += blockDim.x) {
+      const int t = i / KX, k = i - t * KX;
+      const int rr2 = t / 3, j = t - 3 * rr2;
+      const size_t row2 = r0 + rr2;
+      if (row2 >= R) continue;
+      const cx<T> zk = fb[(size_t)t * NX + k], zm = conj(fb[(size_t)t * NX + (NX - k) % NX]);
+      const cx<T> a = (zk + zm) * (T)0.5;
+      const cx<T> d = zk - zm;
+      const int fa = (j == 0) ? 0 : (j == 1 ? 1 : 4);  // tau11 | tau22 | tau13
+      const int fbi = (j == 0) ? 3 : (j == 1 ? 2 : 5); // tau12 | tau33 | tau23
+      th[(size_t)fa * plane + row2 * KX + k] = a;
+      th[(size_t)fbi * plane + row2 * KX + k] = mk(d.y * (T)0.5, -d.x * (T)0.5);
+    }
+    __syncthreads();
+  }
+  (void)failed;
+  for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+  if ((tid & 31) == 0) red[warp] = dsum;
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid == 0) {
+    double sacc = 0.0;
+    for (int w = 0; w < 16; w++) sacc += red[w];
+    dissip_part[blockIdx.x] = sacc;
+  }
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tbase, 256);
+  }
+}
 
 // Mean dissipation (per-CTA sums in CTA order) -> flag and status.
 static __global__ void k_learned_flag(const double* __restrict__ part, int nparts, double inv_n_delta,
@@ -157,8 +275,8 @@ __global__ void k_ldiv(const cx<T>* __restrict__ th, cx<T>* __restrict__ run, cx
   if (ky == NY / 2) return;
   const T xk = (T)(a.kx0 * kx), yk = (T)(a.ky0 * signed_k(ky, NY)), dzm = (T)a.dzm;
   auto tf = [&](int f, int k) -> cx<T> { return th[((size_t)f * NZ + (k - 1)) * nm + m]; };
-  auto t13w = [&](int k) -> cx<T> { return (k >= 1 && k <= NZ - 1) ? (tf(4, k) + tf(4, k + 1)) * (T)0.5 : zero_cx<T>(); };
-  auto t23w = [&](int k) -> cx<T> { return (k >= 1 && k <= NZ - 1) ? (tf(5, k) + tf(5, k + 1)) * (T)0.5 : zero_cx<T>(); };
+  auto t13w = [&](int k) -> cx<T> { return (k >= 2 && k <= NZ - 2) ? (tf(4, k) + tf(4, k + 1)) * (T)0.5 : zero_cx<T>(); };
+  auto t23w = [&](int k) -> cx<T> { return (k >= 2 && k <= NZ - 2) ? (tf(5, k) + tf(5, k + 1)) * (T)0.5 : zero_cx<T>(); };
   const size_t o = (size_t)(z - 1) * nm + m;
   const cx<T> du = mul_i(tf(0, z)) * (-xk) - mul_i(tf(3, z)) * yk - (t13w(z) - t13w(z - 1)) * dzm;
   const cx<T> dv = mul_i(tf(3, z)) * (-xk) - mul_i(tf(1, z)) * yk - (t23w(z) - t23w(z - 1)) * dzm;

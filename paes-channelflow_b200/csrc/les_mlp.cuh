@@ -117,6 +117,103 @@ __device__ __forceinline__ void issue_layer(uint32_t d, uint32_t a_s, uint32_t w
 constexpr int kInferGroups = 4;
 constexpr size_t kInferSmem = sizeof(MlpDev) + (size_t)kInferGroups * 16384 + 256;
 
+// One group's view of its tile: shared-memory addresses of its activation
+// tile and of the weight tiles, its 64 tensor-memory columns, its named
+// barrier and mbarrier, and the mbarrier phase.
+struct MlpGroup {
+  unsigned char* act;
+  uint32_t act_s, w1s, w2s, w3s, w4s, dcol, my_t;
+  int bar;
+  uint64_t* mbar;
+  uint32_t parity;
+};
+
+__device__ __forceinline__ MlpGroup mlp_group(MlpDev* P, unsigned char* act, uint32_t tbase, int g, int q,
+                                              uint64_t* mbar) {
+  MlpGroup G;
+  G.act = act;
+  G.act_s = tc::smem_addr(act);
+  G.w1s = tc::smem_addr(P->w1);
+  G.w2s = tc::smem_addr(P->w2);
+  G.w3s = tc::smem_addr(P->w3);
+  G.w4s = tc::smem_addr(P->w4);
+  G.dcol = tbase + 64 * g;
+  G.my_t = G.dcol + ((uint32_t)(q * 32) << 16);
+  G.bar = 1 + g;
+  G.mbar = mbar;
+  G.parity = 0;
+  return G;
+}
+
+// The network on one 128-sample tile by one group of 4 warps (thread r owns
+// sample r): features f0, f1 (bf16 x 16) in, the 16 output columns of this
+// sample's lane (outputs + b4) out.  Returns false in every thread of the
+// group when an MMA did not complete within its wait limit.
+__device__ __forceinline__ bool mlp_tile(MlpGroup& G, const MlpDev* P, int r, uint4 f0, uint4 f1,
+                                         float (&y)[16]) {
+  auto wait_mma = [&]() -> bool {
+    const bool ok = tc::mbar_wait(G.mbar, G.parity, kMmaWaitNs);
+    G.parity ^= 1;
+    tc::fence_after_sync();
+    return ok;
+  };
+  *reinterpret_cast<uint4*>(G.act + 2 * tc::tile_elem(r, 0, 16)) = f0;
+  *reinterpret_cast<uint4*>(G.act + 2 * tc::tile_elem(r, 8, 16)) = f1;
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  tc::bar_sync(G.bar, 128);
+  if (r == 0) {
+    tc::fence_after_sync();
+    issue_layer<64, 16>(G.dcol, G.act_s, G.w1s);
+    tc::mma_commit(G.mbar);
+  }
+  bool bad = !wait_mma();
+  hidden_epilogue(G.my_t, P->b1, G.act, r);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  if (bar_any(G.bar, 128, bad)) return false;
+  if (r == 0) {
+    tc::fence_after_sync();
+    issue_layer<64, 64>(G.dcol, G.act_s, G.w2s);
+    tc::mma_commit(G.mbar);
+  }
+  bad = !wait_mma();
+  hidden_epilogue(G.my_t, P->b2, G.act, r);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  if (bar_any(G.bar, 128, bad)) return false;
+  if (r == 0) {
+    tc::fence_after_sync();
+    issue_layer<64, 64>(G.dcol, G.act_s, G.w3s);
+    tc::mma_commit(G.mbar);
+  }
+  bad = !wait_mma();
+  hidden_epilogue(G.my_t, P->b3, G.act, r);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  if (bar_any(G.bar, 128, bad)) return false;
+  if (r == 0) {
+    tc::fence_after_sync();
+    issue_layer<16, 64>(G.dcol, G.act_s, G.w4s);
+    tc::mma_commit(G.mbar);
+  }
+  bad = !wait_mma();
+  tc::tmem_ld16(G.my_t, y);
+#pragma unroll
+  for (int j = 0; j < 16; j++) y[j] += P->b4[j];
+  tc::fence_before_sync();
+  return !bar_any(G.bar, 128, bad);
+}
+
+// After a failed tile: flag the error and give the outstanding commit a
+// bounded wait before the tensor memory is released.
+__device__ __forceinline__ void mlp_tile_failed(MlpGroup& G, int r, int* err) {
+  if (r == 0) {
+    atomicOr(err, ERR_MMA_TIMEOUT);
+    tc::mbar_wait(G.mbar, G.parity ^ 1, kMmaWaitNs);
+  }
+}
+
 template <class Out>
 __global__ void __launch_bounds__(128 * kInferGroups, 1)
 k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long long n, Out out,
@@ -142,83 +239,20 @@ k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tbase = *tslot;
-
-  unsigned char* act = act_all + (size_t)g * 16384;
-  const uint32_t act_s = tc::smem_addr(act);
-  const uint32_t w1s = tc::smem_addr(P->w1), w2s = tc::smem_addr(P->w2), w3s = tc::smem_addr(P->w3),
-                 w4s = tc::smem_addr(P->w4);
-  const uint32_t dcol = tbase + 64 * g;
-  const uint32_t my_t = dcol + ((uint32_t)(q * 32) << 16);
-  const int bar = 1 + g;
-  uint32_t parity = 0;
-  bool failed = false;
+  MlpGroup grp = mlp_group(P, act_all + (size_t)g * 16384, tbase, g, q, &bars[g]);
   double dsum = 0.0;
   const long long ntiles = (n + 127) / 128;
-  auto wait_mma = [&]() -> bool {
-    const bool ok = tc::mbar_wait(&bars[g], parity, kMmaWaitNs);
-    parity ^= 1;
-    tc::fence_after_sync();
-    return ok;
-  };
   for (long long tile = (long long)blockIdx.x * G + g; tile < ntiles; tile += (long long)gridDim.x * G) {
     const long long p = tile * 128 + r;
     const bool valid = p < n;
     uint4 f0 = make_uint4(0, 0, 0, 0), f1 = f0;
     if (valid) { f0 = __ldg(feat + 2 * p); f1 = __ldg(feat + 2 * p + 1); }
-    *reinterpret_cast<uint4*>(act + 2 * tc::tile_elem(r, 0, 16)) = f0;
-    *reinterpret_cast<uint4*>(act + 2 * tc::tile_elem(r, 8, 16)) = f1;
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    tc::bar_sync(bar, 128);
-    if (r == 0) {
-      tc::fence_after_sync();
-      issue_layer<64, 16>(dcol, act_s, w1s);
-      tc::mma_commit(&bars[g]);
-    }
-    bool bad = !wait_mma();
-    hidden_epilogue(my_t, P->b1, act, r);
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    if (bar_any(bar, 128, bad)) { failed = true; break; }
-    if (r == 0) {
-      tc::fence_after_sync();
-      issue_layer<64, 64>(dcol, act_s, w2s);
-      tc::mma_commit(&bars[g]);
-    }
-    bad = !wait_mma();
-    hidden_epilogue(my_t, P->b2, act, r);
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    if (bar_any(bar, 128, bad)) { failed = true; break; }
-    if (r == 0) {
-      tc::fence_after_sync();
-      issue_layer<64, 64>(dcol, act_s, w3s);
-      tc::mma_commit(&bars[g]);
-    }
-    bad = !wait_mma();
-    hidden_epilogue(my_t, P->b3, act, r);
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    if (bar_any(bar, 128, bad)) { failed = true; break; }
-    if (r == 0) {
-      tc::fence_after_sync();
-      issue_layer<16, 64>(dcol, act_s, w4s);
-      tc::mma_commit(&bars[g]);
-    }
-    bad = !wait_mma();
     float y[16];
-    tc::tmem_ld16(my_t, y);
-#pragma unroll
-    for (int j = 0; j < 16; j++) y[j] += P->b4[j];
-    dsum += out(p, valid, y, f0, f1, P);
-    tc::fence_before_sync();
-    if (bar_any(bar, 128, bad)) { failed = true; break; }
-  }
-  if (failed) {
-    if (r == 0) {
-      atomicOr(err, ERR_MMA_TIMEOUT);
-      tc::mbar_wait(&bars[g], parity ^ 1, kMmaWaitNs);  // the commit that did not arrive in time
+    if (!mlp_tile(grp, P, r, f0, f1, y)) {
+      mlp_tile_failed(grp, r, err);
+      break;
     }
+    dsum += out(p, valid, y, f0, f1, P);
   }
   // per-CTA dissipation sum, fixed order
   for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);

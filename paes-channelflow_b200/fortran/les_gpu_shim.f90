@@ -1,4 +1,4 @@
-! les_gpu_shim.f90 -- Fortran binding of libles_gpu.so (include/les_gpu.h).
+! les_gpu_shim.f90 -- Fortran binding of libles_gpu.so (include/les_gpu.h, include/les_mlp.h).
 !
 ! Replaces comp1.o comp2.o compadv1.o compsgs1.o compsgs3.o derivs1.o
 ! derivs2.o press.o tridv.o filter_fftw.o lowerbc.o upperbc.o complen.o in
@@ -71,6 +71,33 @@ module les_gpu
        import :: c_ptr, c_int
        type(c_ptr), value :: h, meanbuf, scalars
      end function
+     ! learned closure (include/les_mlp.h): create a network, load the
+     ! parameters of a weights file (params(9478), norm(34) as real(c_float)),
+     ! attach it to a handle configured with imodel = 5
+     integer(c_int) function les_mlp_create(device, m) bind(C, name="les_mlp_create")
+       import :: c_ptr, c_int
+       integer(c_int), value :: device
+       type(c_ptr), intent(out) :: m
+     end function
+     integer(c_int) function les_mlp_set_params(m, params, norm) bind(C, name="les_mlp_set_params")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: m, params, norm
+     end function
+     integer(c_int) function les_gpu_set_mlp(h, m, re_tau) bind(C, name="les_gpu_set_mlp")
+       import :: c_ptr, c_int, c_double
+       type(c_ptr), value :: h, m
+       real(c_double), value :: re_tau
+     end function
+     integer(c_int) function les_gpu_learned_status(h, used, dissipation) bind(C, name="les_gpu_learned_status")
+       import :: c_ptr, c_int, c_double
+       type(c_ptr), value :: h
+       integer(c_int), intent(out) :: used
+       real(c_double), intent(out) :: dissipation
+     end function
+     subroutine les_mlp_destroy(m) bind(C, name="les_mlp_destroy")
+       import :: c_ptr
+       type(c_ptr), value :: m
+     end subroutine
      type(c_ptr) function les_gpu_last_error(h) bind(C, name="les_gpu_last_error")
        import :: c_ptr
        type(c_ptr), value :: h

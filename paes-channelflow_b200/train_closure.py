@@ -30,7 +30,9 @@
 6. A-posteriori (optional): coarse runs from the first filtered snapshot
    with the Deardorff closure and with the network; mean U(z) against the
    filtered fine run's mean profile.
-7. Writes <out>.npz (params, norm, re_tau, grids) and <out>.json (report).
+7. Writes <out>.npz (params, norm, re_tau, grids), <out>.json (report) and
+   <out>_eval.npz (the first filtered snapshot and the filtered fine run's
+   mean profile; --evaluate repeats step 6 from it).
 """
 import argparse
 import importlib.util
@@ -336,8 +338,11 @@ def run(args, log=print):
     rep_ho = apriori(mlp, fho, tho, norm, delta)
     params, _ = mlp.get_params()
     mlp.close()
-    apost = aposteriori(first, info, params, norm, args.aposteriori, log) if args.aposteriori else None
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    # what the a-posteriori runs need, for evaluating later closures without a new fine run
+    ev = dict(coarse=info["coarse"], re_tau=info["re_tau"], z0=info["z0"], filtered_mean_u=info["filtered_mean_u"])
+    np.savez(args.out + "_eval.npz", first=first, meta=json.dumps(ev))
+    apost = aposteriori(first, info, params, norm, args.aposteriori, log) if args.aposteriori else None
     np.savez(args.out + ".npz", params=params, norm=norm, re_tau=np.float64(args.re_tau),
              coarse=np.array(info["coarse"]), fine=np.array(info["fine"]), factor=np.array(info["factor"]))
     report = dict(data=info, training=dict(steps=steps, seconds=secs, batch=args.batch, lr=args.lr,
@@ -349,6 +354,22 @@ def run(args, log=print):
         json.dump(report, fh, indent=1)
     log(json.dumps(rep_ho, indent=1))
     return report
+
+
+def evaluate(args, log=print):
+    """A-posteriori runs only, from <out>.npz (network) and <out>_eval.npz
+    (first filtered snapshot and the filtered fine run's mean profile);
+    updates the 'aposteriori' entry of <out>.json."""
+    z = np.load(args.out + ".npz")
+    ev = np.load(args.out + "_eval.npz")
+    info = json.loads(str(ev["meta"]))
+    apost = aposteriori(ev["first"], info, z["params"], z["norm"], args.aposteriori or 4000, log)
+    rp = args.out + ".json"
+    rep_ = json.load(open(rp)) if os.path.exists(rp) else {}
+    rep_["aposteriori"] = apost
+    with open(rp, "w") as fh:
+        json.dump(rep_, fh, indent=1)
+    return apost
 
 
 def main(argv=None):
@@ -371,8 +392,13 @@ def main(argv=None):
     ap.add_argument("--resolved-only", action="store_true",
                     help="targets without the fine run's own model stress")
     ap.add_argument("--out", default=os.path.join(HERE, "weights", "sgs_c4"))
+    ap.add_argument("--evaluate", action="store_true",
+                    help="only the a-posteriori runs, from <out>.npz and <out>_eval.npz")
     args = ap.parse_args(argv)
-    run(args)
+    if args.evaluate:
+        evaluate(args)
+    else:
+        run(args)
 
 
 if __name__ == "__main__":
