@@ -220,6 +220,29 @@ int les_op_tridv(void* bdar, int ny, int n, int real_bytes, void* stream);
 int les_op_expand_noalloc(const void* xsmall, void* xlarge, int nx, int ny,
                           int howmany, int real_bytes, void* stream);
 
+/* Restart files (read_write.f90:16-40, les.F90:69-82 and 331-351): the
+ * reference's Fortran unformatted sequential ".field" layout, each record
+ * framed by its 4-byte length:
+ *   time, nnx, nny, nnz, xl, yl, zl | dt, z0, utau |
+ *   divgls, fcor, ugtop, ugbot, vgtop, vgbot | then per level iz = 1..nnz:
+ *   u, v, w, e, p(1:nnx,1:nny) of level iz.
+ * real_bytes: 4 for the shipped build, 8 for -fdefault-real-8 (integers are
+ * 4 bytes in both).  divgls..vgbot are written as 0 (not used by this path).
+ *
+ * les_gpu_write_field: downloads the state (synchronous on the device) and
+ * writes the file; with async != 0 the file is written by a host thread and
+ * the call returns once the data are on the host, so the handle can keep
+ * stepping; les_gpu_field_wait joins that thread and returns its status (a
+ * later write, read or finalize also waits for it).
+ * les_gpu_read_field: reads a file of this handle's grid and uploads it
+ * (upload semantics: deal, tendencies untouched); *time = its start time.
+ * les_gpu_field_header: dims[3] and hdr[13] = time, xl, yl, zl, dt, z0,
+ * utau, divgls, fcor, ugtop, ugbot, vgtop, vgbot without a handle. */
+int les_gpu_write_field(les_handle* h, const char* path, double time, int real_bytes, int async);
+int les_gpu_field_wait(les_handle* h);
+int les_gpu_read_field(les_handle* h, const char* path, int real_bytes, double* time);
+int les_gpu_field_header(const char* path, int real_bytes, int* dims, double* hdr);
+
 /* Message of the last failed les_op_* call on this thread. */
 const char* les_op_last_error(void);
 

@@ -110,14 +110,31 @@ def dissipation(g, tau):
     return float(d.mean())
 
 
-def divergence(tau, xl, yl, zl):
-    """Dealiased stress divergence (lru, lrv, lrw), each (nz, ny, nx)."""
+def network_viscosity(g, tau, xkmax):
+    """Face values (index j = w-level j) of the network's effective
+    viscosity: per level -sum(tau13 uz + tau23 vz) / sum(uz^2 + vz^2)
+    clipped to [0, xkmax], averaged over the cells j and j+1."""
+    nz = g.shape[1]
+    a = (tau[4] * g[6] + tau[5] * g[7]).reshape(nz, -1).sum(axis=1)
+    b = (g[6] ** 2 + g[7] ** 2).reshape(nz, -1).sum(axis=1)
+    nuc = np.clip(np.where(b > 0, -a / np.where(b > 0, b, 1.0), 0.0), 0.0, xkmax)
+    out = np.zeros(nz + 1)
+    for j in range(1, nz):
+        out[j] = 0.5 * (nuc[j - 1] + nuc[j])
+    return out
+
+
+def divergence(tau, xl, yl, zl, u=None, v=None, nut=None):
+    """Dealiased stress divergence (lru, lrv, lrw), each (nz, ny, nx).  With
+    u, v and the face viscosity nut (network_viscosity()), the compact-stencil
+    correction -nut(j) (3 (u(j+1) - u(j)) - (u(j+2) - u(j-1))) / (4 dz) is
+    added to tau13, tau23 on the faces 2..nz-2 (it damps odd-even modes)."""
     _, nz, ny, nx = tau.shape
     sp = Spec(nx, ny, xl, yl)
     dz = zl / nz
-    # tau13, tau23 on the w-levels 2..nz-2; the walls and the wall-adjacent
-    # w-levels 1 and nz-1 keep the wall model's and the Deardorff stresses
-    tw = lambda f, k: 0.5 * (tau[f, k - 1] + tau[f, k]) if 2 <= k <= nz - 2 else np.zeros((ny, nx))
+    # tau13, tau23 averaged to the interior w-levels; 0 on the walls (the
+    # wall model's stresses stay in the padded kernels)
+    tw = lambda f, k: 0.5 * (tau[f, k - 1] + tau[f, k]) if 1 <= k <= nz - 1 else np.zeros((ny, nx))
     lru = np.zeros((nz, ny, nx)); lrv = np.zeros_like(lru); lrw = np.zeros_like(lru)
     for k in range(1, nz + 1):
         t = lambda f: tau[f, k - 1]
@@ -125,6 +142,14 @@ def divergence(tau, xl, yl, zl):
         lrv[k - 1] = sp.deal(-sp.dx(t(3)) - sp.dy(t(1)) - (tw(5, k) - tw(5, k - 1)) / dz)
         if k <= nz - 1:
             lrw[k - 1] = sp.deal(-sp.dx(tw(4, k)) - sp.dy(tw(5, k)) - (tau[2, k] - tau[2, k - 1]) / dz)
+    if nut is not None:
+        def tc(a, j):
+            if j < 2 or j > nz - 2:
+                return np.zeros((ny, nx))
+            return -nut[j] * (3 * (a[j] - a[j - 1]) - (a[j + 1] - a[j - 2])) / (4 * dz)
+        for k in range(1, nz + 1):
+            lru[k - 1] -= (tc(u, k) - tc(u, k - 1)) / dz
+            lrv[k - 1] -= (tc(v, k) - tc(v, k - 1)) / dz
     return lru, lrv, lrw
 
 

@@ -679,8 +679,7 @@ struct Les {
   void compsgs1(int iz, int j, int jp1, int k, int km1, int l, int lm1, int lp1, int nm1, int n, int np1,
                 int np2) {
     const T mom = sgs_mom;
-    // the wall-adjacent w-levels 1 and nnz-1 keep their shear stresses
-    const T momw = (iz == 1 || iz == nnz - 1) ? (T)1 : mom;
+    const T momw = mom;
     if (iz == 1) {
       complen(lm1, -1, nm1, n);
       complen(l, 0, n, np1);
@@ -763,9 +762,9 @@ struct Les {
   // stage uses the network when the mean of -tau_ij S_ij is >= 0, and then
   // adds the dealiased stress divergence to ru, rv, rw:
   //   ru += -d/dx tau11 - d/dy tau12 - (tau13w(k) - tau13w(k-1))/dz, ...
-  // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on the w-levels 2..nnz-2 and 0
-  // on the walls and the wall-adjacent w-levels 1 and nnz-1 (the wall model's
-  // and the Deardorff shear stresses stay there in compsgs1).
+  // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on the interior w-levels and 0
+  // on the walls (the wall model's stresses stay in compsgs1), plus the
+  // compact-stencil correction of the shear stresses on the faces 2..nnz-2.
   void learned_prepare() {
     const int NZ = nnz;
     std::vector<std::vector<T>> tau((size_t)6 * (NZ + 2), std::vector<T>(ps, (T)0));
@@ -774,6 +773,7 @@ struct Les {
     std::vector<T> wc(ps);
     const double h = (double)zl / 2.0;
     double dsum_ = 0.0;
+    std::vector<double> nuA((size_t)NZ + 2, 0.0), nuB((size_t)NZ + 2, 0.0);
     for (int iz = 1; iz <= NZ; iz++) {
       sp.xderiv(u.at(iz), g[0].data(), xk.data(), nnx, nny);
       sp.xderiv(v.at(iz), g[1].data(), xk.data(), nnx, nny);
@@ -812,6 +812,8 @@ struct Les {
         const double s12 = 0.5 * ((double)g[3][q] + g[1][q]), s13 = 0.5 * ((double)g[6][q] + g[2][q]),
                      s23 = 0.5 * ((double)g[7][q] + g[5][q]);
         dsum_ += -(t[0] * s11 + t[1] * s22 + t[2] * s33 + 2.0 * (t[3] * s12 + t[4] * s13 + t[5] * s23));
+        nuA[iz] += t[4] * (double)g[6][q] + t[5] * (double)g[7][q];
+        nuB[iz] += (double)g[6][q] * g[6][q] + (double)g[7][q] * g[7][q];
       }
     }
     learned_dissip = dsum_ / ((double)ps * NZ);
@@ -820,7 +822,7 @@ struct Les {
     // stress divergence
     std::vector<T> t13w_m(ps), t13w_p(ps), t23w_m(ps), t23w_p(ps), f1(ps), f2(ps);
     auto tw = [&](int f, int k, std::vector<T>& o) {
-      if (k < 2 || k > NZ - 2) { std::fill(o.begin(), o.end(), (T)0); return; }
+      if (k < 1 || k > NZ - 1) { std::fill(o.begin(), o.end(), (T)0); return; }
       for (size_t q = 0; q < ps; q++) o[q] = (T)0.5 * (TA(f, k)[q] + TA(f, k + 1)[q]);
     };
     for (int iz = 1; iz <= NZ; iz++) {
@@ -843,6 +845,30 @@ struct Les {
         sp.deal(a, nnx, nny);
       } else {
         std::fill_n(a, ps, (T)0);
+      }
+    }
+    // Compact-stencil correction on the learned faces 2..nnz-2 (odd-even
+    // damping): tau13c(j) = -nu(j) D3[u](j), D3[u](j) = (3 (u(j+1) - u(j)) -
+    // (u(j+2) - u(j-1))) / (4 dz); nu(j) the mean of the network's effective
+    // viscosity -sum(tau13 uz + tau23 vz) / sum(uz^2 + vz^2) of the cells j
+    // and j+1, each clipped to [0, xkmax]; the same for v.
+    auto nuc = [&](int k) -> double {
+      double nu = nuB[k] > 0.0 ? -nuA[k] / nuB[k] : 0.0;
+      return std::min(std::max(nu, 0.0), (double)xkmax);
+    };
+    std::vector<T> nut((size_t)NZ + 1, (T)0);
+    for (int j = 2; j <= NZ - 2; j++) nut[j] = (T)(0.5 * (nuc(j) + nuc(j + 1)));
+    auto tc = [&](Levels<T>& f, int j, size_t q) -> T {
+      if (j < 2 || j > NZ - 2) return (T)0;
+      const T d3 = ((T)3 * (f.at(j + 1)[q] - f.at(j)[q]) - (f.at(j + 2)[q] - f.at(j - 1)[q])) * ((T)0.25 * dzm);
+      return -nut[j] * d3;
+    };
+    for (int iz = 1; iz <= NZ; iz++) {
+      T* a = lru.at(iz);
+      T* b = lrv.at(iz);
+      for (size_t q = 0; q < ps; q++) {
+        a[q] -= (tc(u, iz, q) - tc(u, iz - 1, q)) * dzm;
+        b[q] -= (tc(v, iz, q) - tc(v, iz - 1, q)) * dzm;
       }
     }
   }

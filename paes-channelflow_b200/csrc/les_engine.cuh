@@ -187,10 +187,11 @@ struct Engine : EngineBase {
   const MlpDev* mlp = nullptr;
   double re_tau = 0.0;
   int nsm = 148;
-  DevBuf<cx<T>> lgy;   // [9][NZ][NY][KX] gradient spectra along x
-  DevBuf<T> lphys;     // [9][NZ][NY][NX] gradient planes (features, filter); in the stage the
-                       // tau rows th [6][NZ][NY][KX] complex
-  DevBuf<double> lpart, lstat;
+  DevBuf<cx<T>> lgy;   // [6][NZ][NY][KX] rows U, UY, V, VY, W, WY; then the tau rows th
+  DevBuf<T> ltau;      // [8][NZ][NY][NX] tau at the cell centres + viscosity products
+  DevBuf<uint4> lfeat; // [N][16] bf16 features
+  DevBuf<float> fraw;  // [N][16] raw f32 features (training data)
+  DevBuf<double> lpart, lstat, lnut;
   DevBuf<int> lflag;
   DevBuf<T> fscr, fcp;      // filter scratch: z-averaged fine planes, coarse planes
   DevBuf<cx<T>> fsh, fch;   // filter scratch: fine and coarse spectra
@@ -253,7 +254,7 @@ struct Engine : EngineBase {
     clipflag.release(); ephys.release(); dEX.release(); dEY.release(); wallpl.release();
     for (auto& b : xout) b.release();
     for (auto& b : phys) b.release();
-    lgy.release(); lphys.release(); lpart.release(); lstat.release(); lflag.release();
+    lgy.release(); ltau.release(); lfeat.release(); fraw.release(); lpart.release(); lnut.release(); lstat.release(); lflag.release();
     fscr.release(); fcp.release(); fsh.release(); fch.release();
   }
   cudaStream_t stream() override { return st; }
@@ -466,9 +467,11 @@ struct Engine : EngineBase {
   bool learned_on() const { return mlp != nullptr && cfg.imodel == LES_SGS_LEARNED; }
   void learned_alloc() {
     if (lgy.p) return;
-    lgy.alloc(9 * nm * NZ);
-    lphys.alloc(9 * ps * NZ);
+    lgy.alloc(6 * nm * NZ);
+    ltau.alloc(8 * ps * NZ);
+    lfeat.alloc(2 * ps * NZ);
     lpart.alloc(nsm);
+    lnut.alloc((size_t)NZ * kNuChunks * 2);
     lstat.alloc(2);
     lflag.alloc(1);
   }
@@ -490,30 +493,33 @@ struct Engine : EngineBase {
     if (used) *used = (int)v[1];
     if (dissipation) *dissipation = v[0];
   }
-  // the nine gradient planes at the cell centres (lphys [9][N])
-  void learned_gradients() {
+  // y-inverse rows of the velocity spectra, then gradients and features
+  // at the cell centres (bf16 normalised by the attached network, or raw f32)
+  void learned_features_into(void* feat, bool raw, double rt) {
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = ColCfg<NN, T>;
-      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC), NZ, 9), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
-             (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)kx0, (T)ky0, (T)dzm, tw);
+      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC), NZ, 6), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
+             (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)ky0, tw);
     });
+    const T zpl = (T)(rt / (cfg.zl / 2.0));
     with_small(NX, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
-      using C = RowCfg<NN>;
-      const size_t nrows = 9 * (size_t)NZ * NY;
-      launch(k_row_c2r<T, NN>, dim3(cdiv((nrows + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
-             (const cx<T>*)lgy.p, lphys.p, (int)nrows, KX, tw);
+      using L = LgxCfg<NN>;
+      const unsigned grid = cdiv((size_t)NZ * NY, L::RB);
+      if (raw)
+        launch(k_lgrad_x<T, NN, true>, dim3(grid), dim3(L::THREADS), L::template smem<T>(), st, (const cx<T>*)lgy.p,
+               feat, mlp, NY, NZ, (T)kx0, (T)dzm, (T)dsl, (T)dz, (T)cfg.zl, zpl, tw);
+      else
+        launch(k_lgrad_x<T, NN, false>, dim3(grid), dim3(L::THREADS), L::template smem<T>(), st, (const cx<T>*)lgy.p,
+               feat, mlp, NY, NZ, (T)kx0, (T)dzm, (T)dsl, (T)dz, (T)cfg.zl, zpl, tw);
     });
   }
   // raw (unnormalised) features of the current state, f32 [N][16]
   void learned_features(double rt, float* feat) override {
     if (phase != 0) throw std::logic_error("learned_features inside a split comp1..comp2 sequence");
     learned_alloc();
-    learned_gradients();
-    const size_t N = ps * NZ;
-    launch(k_lfeat_raw<T>, dim3(cdiv(N, 256)), dim3(256), 0, st, (const T*)lphys.p, (float4*)feat, (long long)N,
-           (long long)ps, (T)dsl, (T)dz, (T)cfg.zl, (T)(rt / (cfg.zl / 2.0)));
+    learned_features_into(feat, true, rt);
   }
   // explicit filter of the current state onto the grid (NX/fxy, NY/fxy, NZ/fz)
   void learn_filter(int fxy, int fz, int with_model, double* out) override {
@@ -530,13 +536,14 @@ struct Engine : EngineBase {
     if (fcp.n < npl * psc) { fcp.release(); fcp.alloc(npl * psc); }
     if (with_model) {
       learned_alloc();
-      learned_gradients();
+      if (fraw.n < 16 * ps * NZ) { fraw.release(); fraw.alloc(16 * ps * NZ); }
+      learned_features_into(fraw.p, true, 1.0);  // the gradients (columns 0..8) do not depend on re_tau
     }
     to_physical(uh.p, phys[0].p, NZ);
     to_physical(vh.p, phys[1].p, NZ);
     to_physical(wh.p, phys[2].p, NZ);
     launch(k_filt_z<T>, dim3(cdiv(ps, 256), NZc), dim3(256), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
-           (const T*)phys[2].p, with_model ? (const T*)lphys.p : (const T*)nullptr, (const T*)e.p, (T)dsl,
+           (const T*)phys[2].p, with_model ? (const float*)fraw.p : (const float*)nullptr, (const T*)e.p, (T)dsl,
            (T)cfg.emin, fscr.p, (long long)ps, NZ, NZc, fz);
     with_small(NX, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
@@ -569,37 +576,33 @@ struct Engine : EngineBase {
   // gradients -> features -> network -> tau and the fallback flag
   void learned_pre() {
     const size_t N = ps * NZ;
-    // gradient spectra along x at every level (lgy [9][NZ][NY][KX])
-    with_small(NY, [&](auto cn) {
-      constexpr int NN = decltype(cn)::value;
-      using C = ColCfg<NN, T>;
-      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC), NZ, 9), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
-             (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)kx0, (T)ky0, (T)dzm, tw);
-    });
-    // x transforms, features, network, tau rows (th = lphys storage as [6][NZ][NY][KX] complex)
-    const double h = cfg.zl / 2.0;
-    int grid = 1;
-    with_small(NX, [&](auto cn) {
-      constexpr int NN = decltype(cn)::value;
-      using L = LearnedRow<NN>;
-      grid = (int)std::min<size_t>(cdiv((size_t)NZ * NY, L::RB), (size_t)nsm);
-      launch(k_learned_row<T, NN>, dim3(grid), dim3(512), L::template smem<T>(), st, mlp, (const cx<T>*)lgy.p,
-             (cx<T>*)lphys.p, NY, NZ, (T)dsl, (T)dz, (T)cfg.zl, (T)(re_tau / h), tw, lpart.p, err.p);
-    });
+    learned_features_into(lfeat.p, false, re_tau);
+    const long long ntiles = ((long long)N + 127) / 128;
+    const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, nsm);
+    MlpOutTau<T> out{ltau.p, (long long)N};
+    launch(k_mlp_infer<MlpOutTau<T>>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, st, mlp,
+           (const uint4*)lfeat.p, (long long)N, out, lpart.p, err.p);
     launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, 1.0 / ((double)N * dsl), lflag.p,
            lstat.p);
   }
-  // tau^ and its divergence into the new tendencies
+  // tau^ and its divergence into the new tendencies (th reuses lgy)
   void learned_post(const StageArgs& a) {
-    cx<T>* th = (cx<T>*)lphys.p;
+    with_small(NX, [&](auto cn) {
+      constexpr int NN = decltype(cn)::value;
+      using C = RowCfg<NN>;
+      const size_t nrows = 6 * (size_t)NZ * NY;
+      launch(k_row_r2c<T, NN>, dim3(cdiv((nrows + 1) / 2, C::NT)), dim3(C::THREADS), C::template smem<T>(), st,
+             (const T*)ltau.p, lgy.p, (int)nrows, KX, tw);
+    });
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = ColCfg<NN, T>;
       launch(k_col_small<T, NN, false>, dim3(cdiv(KX, C::TC), 6 * NZ), dim3(C::THREADS), C::buf(), st,
-             (const cx<T>*)th, th, KX, (T)(1.0 / ((double)NX * NY)), tw);
+             (const cx<T>*)lgy.p, lgy.p, KX, (T)(1.0 / ((double)NX * NY)), tw);
     });
-    launch(k_ldiv<T>, dim3(cdiv(nm, 128), NZ), dim3(128), 0, st, (const cx<T>*)th, run.p, rvn.p, rwn.p,
-           (const int*)lflag.p, a);
+    launch(k_learned_nu<T>, dim3(NZ, kNuChunks), dim3(256), 0, st, (const T*)ltau.p, lnut.p, ps, (long long)(ps * NZ));
+    launch(k_ldiv<T>, dim3(cdiv(nm, 128), NZ), dim3(128), 0, st, (const cx<T>*)lgy.p, run.p, rvn.p, rwn.p,
+           (const cx<T>*)uh.p, (const cx<T>*)vh.p, (const double*)lnut.p, (const int*)lflag.p, a);
   }
   // Wall-model plane sums from the physical U, V rows of levels 1 and nnz.
   void wall_params_from(const T* U, const T* V, size_t upper_off, const StageArgs& a) {

@@ -248,12 +248,9 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   const T kx0 = (T)a.kx0, dzm = (T)a.dzm, todzm = (T)a.todzm, emin = (T)a.emin;
   const T xkmax = (T)a.xkmax, nu = (T)a.nu, c01 = (T)0.1 * (T)a.dsl;
   const WallParams& wp = *f.wp;
-  // weight of the interior momentum stresses (0 when the learned closure
-  // supplies them); the shear stresses of the wall-adjacent w-levels 1 and
-  // nnz-1 always stay (the learned closure leaves those rows to the wall
-  // model's neighbourhood, like the wall rows themselves)
+  // weight of the interior momentum stresses: 0 when the learned closure
+  // supplies them (the wall rows stay)
   const T mom = (f.lflag && f.lflag[0]) ? (T)0 : (T)1;
-  auto momw = [&](int zw) -> T { return (zw == 1 || zw == NZ - 1) ? (T)1 : mom; };
 
   auto mixrow = [&](int j, int z) -> const cx<T>* {
     return reinterpret_cast<const cx<T>*>(f.in.p[j]) + ((size_t)(z - 1) * MY + y) * KX;
@@ -321,7 +318,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   } else {
     for (int x = threadIdx.x; x < MX; x += blockDim.x) {
       cx<T> uvm = UVs(sm1)[S(x)], uv0 = UVs(s0)[S(x)], wxy = work[0][S(x)];
-      T xk = momw(z0 - 1) * xkk(WEs(sm1)[S(x)].y);
+      T xk = mom * xkk(WEs(sm1)[S(x)].y);
       T uz = (uv0.x - uvm.x) * dzm, vz = (uv0.y - uvm.y) * dzm;
       carry[x] = mk(-xk * (uz + wxy.x), -xk * (vz + wxy.y));
     }
@@ -374,7 +371,6 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
     work[4] = UVs(sm1);
     work[5] = WEs(sm1);
     const bool top = (z == NZ);
-    const T mw = momw(z);
     const bool clip = (!top) && f.clipflag[le - 1];
     const T* dEX = reinterpret_cast<const T*>(f.dEX) + ((size_t)(le - 1) * MY + y) * MX;
     const T* dEY = reinterpret_cast<const T*>(f.dEY) + ((size_t)(le - 1) * MY + y) * MX;
@@ -396,8 +392,8 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
         wall_stress<T>(wp.w[1], wp, a, 1, U0, V0, tuw0, tvw0);
       } else {
         const T uz = (U1 - U0) * dzm, vz = (V1 - V0) * dzm;
-        tuw0 = -mw * xk0 * (uz + wxy.x);
-        tvw0 = -mw * xk0 * (vz + wxy.y);
+        tuw0 = -mom * xk0 * (uz + wxy.x);
+        tvw0 = -mom * xk0 * (vz + wxy.y);
       }
       const T wz0 = (W0 - Wm) * dzm;
       const T tww0 = -s * wz0;

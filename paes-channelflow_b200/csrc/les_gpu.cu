@@ -3,6 +3,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <initializer_list>
+#include <vector>
 #include <functional>
 #include <memory>
 #include <mutex>
@@ -90,12 +93,20 @@ void set_smem_limit(const void* func, size_t bytes) {
 
 using namespace les;
 
+// A restart file written by a host thread while the handle keeps running.
+struct FieldJob {
+  std::thread th;
+  int rc = LES_OK;
+  std::string err;
+};
+
 struct les_handle {
   les_config cfg;
   int device = 0;
   std::unique_ptr<EngineBase> eng;
   std::string err;
   long long launches = 0;
+  std::unique_ptr<FieldJob> fjob;
 };
 
 namespace {
@@ -259,6 +270,7 @@ int les_gpu_init(const les_config* cfg, les_handle** out) {
 
 void les_gpu_finalize(les_handle* h) {
   if (!h) return;
+  if (h->fjob && h->fjob->th.joinable()) h->fjob->th.join();
   {
     DeviceGuard g(h->device);
     h->eng.reset();
@@ -489,5 +501,181 @@ extern "C" int les_gpu_learned_features(les_handle* h, double re_tau, float* fea
   return guarded(h, [&] {
     h->eng->learned_features(re_tau, feat);
     LES_CUDA(cudaStreamSynchronize(h->eng->stream()));
+  });
+}
+
+// ---- restart files (read_write.f90, les.F90:69-82, 331-351) ----
+// Fortran unformatted sequential records, each framed by its byte length
+// as a 4-byte integer before and after it:
+//   1: time, nnx, nny, nnz, xl, yl, zl      (reals, integers as 4 bytes)
+//   2: dt, z0, utau                         (write_params)
+//   3: divgls, fcor, ugtop, ugbot, vgtop, vgbot
+//   3+iz, iz = 1..nnz: u, v, w, e, p(1:nnx,1:nny) of level iz (sav_field)
+// Reals are real_bytes wide: 4 for the shipped build, 8 for -fdefault-real-8.
+namespace {
+
+struct Part { const void* p; size_t n; };
+
+bool write_record(FILE* f, std::initializer_list<Part> parts) {
+  size_t total = 0;
+  for (const Part& q : parts) total += q.n;
+  if (total > 0x7fffffffu) return false;
+  const int32_t m = (int32_t)total;
+  if (fwrite(&m, 4, 1, f) != 1) return false;
+  for (const Part& q : parts)
+    if (q.n && fwrite(q.p, 1, q.n, f) != q.n) return false;
+  return fwrite(&m, 4, 1, f) == 1;
+}
+
+// reads one record of exactly `n` bytes into dst
+bool read_record(FILE* f, void* dst, size_t n) {
+  int32_t m0 = 0, m1 = 0;
+  if (fread(&m0, 4, 1, f) != 1 || (size_t)m0 != n) return false;
+  if (n && fread(dst, 1, n, f) != n) return false;
+  return fread(&m1, 4, 1, f) == 1 && m1 == m0;
+}
+
+void put_real(std::vector<unsigned char>& b, double v, int rb) {
+  const size_t o = b.size();
+  b.resize(o + rb);
+  if (rb == 8) std::memcpy(b.data() + o, &v, 8);
+  else { const float x = (float)v; std::memcpy(b.data() + o, &x, 4); }
+}
+double get_real(const unsigned char* b, int rb) {
+  if (rb == 8) { double v; std::memcpy(&v, b, 8); return v; }
+  float x; std::memcpy(&x, b, 4); return (double)x;
+}
+
+// header records 1-3 -> dims, hdr[13] = time, xl, yl, zl, dt, z0, utau, divgls, fcor, ugtop, ugbot, vgtop, vgbot
+int read_header(FILE* f, int rb, int* dims, double* hdr, std::string& why) {
+  std::vector<unsigned char> r1(4 * rb + 12), r2(3 * rb), r3(6 * rb);
+  if (!read_record(f, r1.data(), r1.size()) || !read_record(f, r2.data(), r2.size()) ||
+      !read_record(f, r3.data(), r3.size())) {
+    why = "not a .field file with real_bytes = " + std::to_string(rb);
+    return LES_EINVAL;
+  }
+  hdr[0] = get_real(r1.data(), rb);
+  std::memcpy(dims, r1.data() + rb, 12);
+  for (int i = 0; i < 3; i++) hdr[1 + i] = get_real(r1.data() + rb + 12 + i * rb, rb);
+  for (int i = 0; i < 3; i++) hdr[4 + i] = get_real(r2.data() + i * rb, rb);
+  for (int i = 0; i < 6; i++) hdr[7 + i] = get_real(r3.data() + i * rb, rb);
+  return LES_OK;
+}
+
+}  // namespace
+
+extern "C" int les_gpu_field_header(const char* path, int real_bytes, int* dims, double* hdr) {
+  if (!path || !dims || !hdr || (real_bytes != 4 && real_bytes != 8)) return LES_EINVAL;
+  FILE* f = fopen(path, "rb");
+  if (!f) { g_static_err = std::string("cannot open ") + path; return LES_EINVAL; }
+  std::string why;
+  const int rc = read_header(f, real_bytes, dims, hdr, why);
+  fclose(f);
+  if (rc) g_static_err = why;
+  return rc;
+}
+
+extern "C" int les_gpu_field_wait(les_handle* h) {
+  if (!h) return LES_EINVAL;
+  if (!h->fjob) return LES_OK;
+  if (h->fjob->th.joinable()) h->fjob->th.join();
+  const int rc = h->fjob->rc;
+  if (rc) h->err = h->fjob->err;
+  h->fjob.reset();
+  return rc;
+}
+
+extern "C" int les_gpu_write_field(les_handle* h, const char* path, double time, int real_bytes, int async) {
+  if (!h || !path || (real_bytes != 4 && real_bytes != 8)) return LES_EINVAL;
+  int rc = les_gpu_field_wait(h);  // one file at a time
+  if (rc) return rc;
+  const les_config c = h->cfg;
+  const size_t ps = (size_t)c.nnx * c.nny, n = ps * c.nnz, bytes = n * real_bytes;
+  unsigned char* buf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  double utau = 0.0;
+  rc = guarded(h, [&] {
+    std::vector<double> mb((size_t)19 * c.nnz), sc(5);
+    h->eng->stats(mb.data(), sc.data());
+    utau = sc[0];
+    for (auto& b : buf) LES_CUDA(cudaMallocHost((void**)&b, bytes));
+    h->eng->download(buf[0], buf[1], buf[2], buf[3], buf[4], real_bytes);
+  });
+  if (rc) {
+    for (auto& b : buf) if (b) cudaFreeHost(b);
+    return rc;
+  }
+  std::unique_ptr<FieldJob> job(new FieldJob());
+  FieldJob* jp = job.get();
+  const std::string fname(path);
+  auto work = [=]() {
+    FILE* f = fopen(fname.c_str(), "wb");
+    bool ok = f != nullptr;
+    if (ok) {
+      const int rb = real_bytes;
+      std::vector<unsigned char> r1, r2, r3;
+      put_real(r1, time, rb);
+      const int32_t d[3] = {c.nnx, c.nny, c.nnz};
+      const size_t o = r1.size();
+      r1.resize(o + 12);
+      std::memcpy(r1.data() + o, d, 12);
+      put_real(r1, c.xl, rb); put_real(r1, c.yl, rb); put_real(r1, c.zl, rb);
+      put_real(r2, c.dt, rb); put_real(r2, c.z0, rb); put_real(r2, utau, rb);
+      for (int i = 0; i < 6; i++) put_real(r3, 0.0, rb);  // divgls, fcor, ugtop, ugbot, vgtop, vgbot
+      ok = write_record(f, {{r1.data(), r1.size()}}) && write_record(f, {{r2.data(), r2.size()}}) &&
+           write_record(f, {{r3.data(), r3.size()}});
+      const size_t pl = ps * rb;
+      for (int iz = 0; ok && iz < c.nnz; iz++) {
+        const size_t off = (size_t)iz * pl;
+        ok = write_record(f, {{buf[0] + off, pl}, {buf[1] + off, pl}, {buf[2] + off, pl}, {buf[3] + off, pl},
+                              {buf[4] + off, pl}});
+      }
+      ok = (fclose(f) == 0) && ok;
+    }
+    for (auto b : buf) cudaFreeHost(b);
+    if (!ok) {
+      jp->rc = LES_EINVAL;
+      jp->err = "writing " + fname + " failed";
+    }
+  };
+  if (async) {
+    job->th = std::thread(work);
+    h->fjob = std::move(job);
+    return LES_OK;
+  }
+  work();
+  rc = job->rc;
+  if (rc) h->err = job->err;
+  return rc;
+}
+
+extern "C" int les_gpu_read_field(les_handle* h, const char* path, int real_bytes, double* time) {
+  if (!h || !path || (real_bytes != 4 && real_bytes != 8)) return LES_EINVAL;
+  int rc = les_gpu_field_wait(h);
+  if (rc) return rc;
+  FILE* f = fopen(path, "rb");
+  if (!f) { h->err = std::string("cannot open ") + path; return LES_EINVAL; }
+  int dims[3];
+  double hdr[13];
+  rc = read_header(f, real_bytes, dims, hdr, h->err);
+  if (!rc && (dims[0] != h->cfg.nnx || dims[1] != h->cfg.nny || dims[2] != h->cfg.nnz)) {
+    h->err = "restart file grid differs from the handle's";
+    rc = LES_EINVAL;
+  }
+  if (rc) { fclose(f); return rc; }
+  const size_t ps = (size_t)dims[0] * dims[1], n = ps * dims[2], pl = ps * real_bytes;
+  std::vector<unsigned char> a[5], rec(5 * pl);
+  for (auto& v : a) v.resize(n * real_bytes);
+  for (int iz = 0; iz < dims[2]; iz++) {
+    if (!read_record(f, rec.data(), rec.size())) {
+      fclose(f);
+      h->err = "restart file is truncated or has another layout";
+      return LES_EINVAL;
+    }
+    for (int q = 0; q < 5; q++) std::memcpy(a[q].data() + (size_t)iz * pl, rec.data() + q * pl, pl);
+  }
+  fclose(f);
+  if (time) *time = hdr[0];
+  return guarded(h, [&] {
+    h->eng->upload(a[0].data(), a[1].data(), a[2].data(), a[3].data(), a[4].data(), real_bytes);
   });
 }

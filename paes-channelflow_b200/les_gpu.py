@@ -133,6 +133,10 @@ def lib():
         "les_gpu_set_mlp": (I, [H, VP, D]),
         "les_gpu_learned_status": (I, [H, ctypes.POINTER(I), ctypes.POINTER(D)]),
         "les_gpu_learn_filter": (I, [H, I, I, I, VP]),
+        "les_gpu_write_field": (I, [H, ctypes.c_char_p, D, I, I]),
+        "les_gpu_field_wait": (I, [H]),
+        "les_gpu_read_field": (I, [H, ctypes.c_char_p, I, ctypes.POINTER(D)]),
+        "les_gpu_field_header": (I, [ctypes.c_char_p, I, ctypes.POINTER(I), ctypes.POINTER(D)]),
         "les_gpu_learned_features": (I, [H, D, VP]),
     }
     for name, (res, args) in sig.items():
@@ -305,6 +309,19 @@ class LesGpu:
         out = torch.empty((c.nnx * c.nny * c.nnz, 16), dtype=torch.float32, device="cuda:%d" % c.device)
         self._check(lib().les_gpu_learned_features(self.h, re_tau, out.data_ptr()))
         return out
+
+    def write_field(self, path, time=0.0, real_bytes=8, background=False):
+        """Restart file in the reference's .field layout (read_write.f90)."""
+        self._check(lib().les_gpu_write_field(self.h, os.fsencode(path), time, real_bytes, int(background)))
+
+    def field_wait(self):
+        self._check(lib().les_gpu_field_wait(self.h))
+
+    def read_field(self, path, real_bytes=8):
+        """Load a restart file of this grid; returns its start time."""
+        t = ctypes.c_double()
+        self._check(lib().les_gpu_read_field(self.h, os.fsencode(path), real_bytes, ctypes.byref(t)))
+        return t.value
 
     def sync(self, timeout_s=60.0):
         self._check(lib().les_gpu_sync(self.h, timeout_s))
@@ -526,3 +543,14 @@ def to_target(t):
     o = torch.zeros((t.shape[0], 8), dtype=torch.float32)
     o[:, :MLP_NOUT] = t
     return o.cuda()
+
+
+def field_header(path, real_bytes=8):
+    """(nnx, nny, nnz), dict of the 13 header values of a restart file."""
+    dims = (ctypes.c_int * 3)()
+    hdr = (ctypes.c_double * 13)()
+    rc = lib().les_gpu_field_header(os.fsencode(path), real_bytes, dims, hdr)
+    if rc != LES_OK:
+        raise LesError(rc, lib().les_gpu_last_error(None).decode())
+    keys = ("time", "xl", "yl", "zl", "dt", "z0", "utau", "divgls", "fcor", "ugtop", "ugbot", "vgtop", "vgbot")
+    return tuple(dims), dict(zip(keys, list(hdr)))

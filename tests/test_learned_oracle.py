@@ -20,6 +20,7 @@ def make_case(sign):
     o.make_ic(seed=3, amp=0.3, re_tau=RE_TAU)
     o.dt_used = o.cfl_dt(0.5)
     o.set_dt(o.dt_used)
+    cfg.dt = o.dt_used
     fl = o.get_fields()
     P = O.mlp_init(seed=31)
     N = np.concatenate([np.zeros(11), np.full(9, 30.0), [2.0 / RE_TAU, 0.0], np.full(6, sign * 1e-3), np.zeros(6)])
@@ -32,7 +33,9 @@ def np_learned(cfg, fl, P, N):
     y = LN.mlp(P, (f - N[:11]) * N[11:22])
     tau = (y * N[22:28] + N[28:34]).T.reshape(6, NZ, NY, NX)
     g = LN.gradients(u, v, w, cfg.xl, cfg.yl, cfg.zl)
-    return LN.dissipation(g, tau), LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl)
+    dz = cfg.zl / NZ
+    nut = LN.network_viscosity(g, tau, dz * dz / cfg.dt / 5.0)
+    return LN.dissipation(g, tau), LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl, u, v, nut)
 
 
 @pytest.mark.parametrize("sign", [1.0, -1.0])
