@@ -471,7 +471,7 @@ struct Engine : EngineBase {
     ltau.alloc(8 * ps * NZ);
     lfeat.alloc(2 * ps * NZ);
     lpart.alloc(nsm);
-    lnut.alloc((size_t)NZ * kNuChunks * 2);
+    lnut.alloc((size_t)NZ * kNuChunks * 2 + NZ + 1);  // partial sums, then the face values
     lstat.alloc(2);
     lflag.alloc(1);
   }
@@ -601,8 +601,10 @@ struct Engine : EngineBase {
              (const cx<T>*)lgy.p, lgy.p, KX, (T)(1.0 / ((double)NX * NY)), tw);
     });
     launch(k_learned_nu<T>, dim3(NZ, kNuChunks), dim3(256), 0, st, (const T*)ltau.p, lnut.p, ps, (long long)(ps * NZ));
+    double* nuf = lnut.p + (size_t)NZ * kNuChunks * 2;
+    launch(k_learned_nu_face, dim3(1), dim3(256), 0, st, (const double*)lnut.p, nuf, NZ, dsl, a.xkmax);
     launch(k_ldiv<T>, dim3(cdiv(nm, 128), NZ), dim3(128), 0, st, (const cx<T>*)lgy.p, run.p, rvn.p, rwn.p,
-           (const cx<T>*)uh.p, (const cx<T>*)vh.p, (const double*)lnut.p, (const int*)lflag.p, a);
+           (const cx<T>*)uh.p, (const cx<T>*)vh.p, (const double*)nuf, (const int*)lflag.p, a);
   }
   // Wall-model plane sums from the physical U, V rows of levels 1 and nnz.
   void wall_params_from(const T* U, const T* V, size_t upper_off, const StageArgs& a) {

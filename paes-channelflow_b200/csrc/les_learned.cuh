@@ -180,7 +180,7 @@ template <class T> struct MlpOutTau {
                         bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
     float g[9];
 #pragma unroll
-    for (int j = 0; j < 9; j++) g[j] = q[j] / P->in_scale[j] + P->in_shift[j];  // d_i u_j * Delta
+    for (int j = 0; j < 9; j++) g[j] = q[j] * P->in_rscale[j] + P->in_shift[j];  // d_i u_j * Delta
     tau[(size_t)6 * N + p] = (T)(t[4] * g[6] + t[5] * g[7]);
     tau[(size_t)7 * N + p] = (T)(g[6] * g[6] + g[7] * g[7]);
     const float s11 = g[0], s22 = g[4], s33 = g[8];
@@ -230,6 +230,31 @@ __global__ void k_learned_nu(const T* __restrict__ tau, double* __restrict__ par
   }
 }
 
+// Face viscosity nu[j], j = 0..NZ, from the partial sums (chunk order):
+// cell values -sum A / sum B * Delta clipped to [0, xkmax], face j = mean of
+// cells j and j+1 (0 outside 2..NZ-2, where no correction is applied).
+static __global__ void k_learned_nu_face(const double* __restrict__ part, double* __restrict__ nuf, int NZ,
+                                         double dsl, double xkmax) {
+  for (int j = threadIdx.x; j <= NZ; j += blockDim.x) {
+    double v = 0.0;
+    if (j >= 2 && j <= NZ - 2) {
+      double c[2];
+      for (int i = 0; i < 2; i++) {
+        const int k = j + i;  // cells j, j+1 (1-based)
+        double sa = 0.0, sb = 0.0;
+        for (int q = 0; q < kNuChunks; q++) {
+          sa += part[((size_t)(k - 1) * kNuChunks + q) * 2];
+          sb += part[((size_t)(k - 1) * kNuChunks + q) * 2 + 1];
+        }
+        double nu = sb > 0.0 ? -sa / sb * dsl : 0.0;
+        c[i] = nu < 0.0 ? 0.0 : (nu > xkmax ? xkmax : nu);
+      }
+      v = 0.5 * (c[0] + c[1]);
+    }
+    nuf[j] = v;
+  }
+}
+
 // Stress divergence of the network's tau (spectral, all levels) into the
 // new tendencies, when the stage uses the network.  On the faces 2..nnz-2
 // (where the stencil fits) the shear stresses get the compact-stencil correction
@@ -242,7 +267,7 @@ __global__ void k_learned_nu(const T* __restrict__ tau, double* __restrict__ par
 template <class T>
 __global__ void k_ldiv(const cx<T>* __restrict__ th, cx<T>* __restrict__ run, cx<T>* __restrict__ rvn,
                        cx<T>* __restrict__ rwn, const cx<T>* __restrict__ uh, const cx<T>* __restrict__ vh,
-                       const double* __restrict__ nupart, const int* __restrict__ flag, StageArgs a) {
+                       const double* __restrict__ nuf, const int* __restrict__ flag, StageArgs a) {
   if (!flag[0]) return;
   const int KX = a.KX, NY = a.NY, NZ = a.NZ;
   const int nm = KX * NY;
@@ -257,19 +282,10 @@ __global__ void k_ldiv(const cx<T>* __restrict__ th, cx<T>* __restrict__ run, cx
   auto t23w = [&](int k) -> cx<T> { return (k >= 1 && k <= NZ - 1) ? (tf(5, k) + tf(5, k + 1)) * (T)0.5 : zero_cx<T>(); };
   const size_t o = (size_t)(z - 1) * nm + m;
   auto lv = [&](const cx<T>* f, int k) -> cx<T> { return f[(size_t)(k - 1) * nm + m]; };
-  auto nuc = [&](int k) -> double {  // cell-centre effective viscosity of level k
-    double sa = 0.0, sb = 0.0;
-    for (int c = 0; c < kNuChunks; c++) {
-      sa += nupart[((size_t)(k - 1) * kNuChunks + c) * 2];
-      sb += nupart[((size_t)(k - 1) * kNuChunks + c) * 2 + 1];
-    }
-    double nu = sb > 0.0 ? -sa / sb * a.dsl : 0.0;
-    return nu < 0.0 ? 0.0 : (nu > a.xkmax ? a.xkmax : nu);
-  };
   auto tc = [&](const cx<T>* f, int j) -> cx<T> {
     if (j < 2 || j > NZ - 2) return zero_cx<T>();
     const cx<T> d3 = ((lv(f, j + 1) - lv(f, j)) * (T)3 - (lv(f, j + 2) - lv(f, j - 1))) * ((T)0.25 * dzm);
-    return d3 * (T)(-0.5 * (nuc(j) + nuc(j + 1)));
+    return d3 * (T)(-nuf[j]);
   };
   const cx<T> du = mul_i(tf(0, z)) * (-xk) - mul_i(tf(3, z)) * yk - (t13w(z) - t13w(z - 1)) * dzm -
                    (tc(uh, z) - tc(uh, z - 1)) * dzm;

@@ -81,7 +81,11 @@ void pack_params(const float* p, const float* norm, MlpDev& d) {
     for (int k = 0; k < 64; k++) d.w4[tc::tile_elem(o, k, 64)] = __float2bfloat16_rn(p[kPW4 + o * 64 + k]);
   for (int i = 0; i < 64; i++) { d.b1[i] = p[kPB1 + i]; d.b2[i] = p[kPB2 + i]; d.b3[i] = p[kPB3 + i]; }
   for (int i = 0; i < kMlpOut; i++) d.b4[i] = p[kPB4 + i];
-  for (int i = 0; i < kMlpIn; i++) { d.in_shift[i] = norm[i]; d.in_scale[i] = norm[kMlpIn + i]; }
+  for (int i = 0; i < kMlpIn; i++) {
+    d.in_shift[i] = norm[i];
+    d.in_scale[i] = norm[kMlpIn + i];
+    d.in_rscale[i] = norm[kMlpIn + i] != 0.f ? 1.f / norm[kMlpIn + i] : 0.f;
+  }
   for (int i = 0; i < kMlpOut; i++) {
     d.out_scale[i] = norm[2 * kMlpIn + i];
     d.out_shift[i] = norm[2 * kMlpIn + kMlpOut + i];

@@ -43,6 +43,7 @@ struct MlpDev {
   __nv_bfloat16 w4[16 * 64];
   float b1[64], b2[64], b3[64], b4[16];
   float in_shift[16], in_scale[16], out_scale[8], out_shift[8];
+  float in_rscale[16];  // 1 / in_scale (0 where in_scale is 0)
 };
 static_assert(sizeof(MlpDev) % 16 == 0, "MlpDev is copied in 16-byte words");
 
