@@ -470,7 +470,7 @@ struct Engine : EngineBase {
     lgy.alloc(6 * nm * NZ);
     ltau.alloc(8 * ps * NZ);
     lfeat.alloc(2 * ps * NZ);
-    lpart.alloc(nsm);
+    lpart.alloc((size_t)nsm * kInferCtasPerSm);
     lnut.alloc((size_t)NZ * kNuChunks * 2 + NZ + 1);  // partial sums, then the face values
     lstat.alloc(2);
     lflag.alloc(1);
@@ -578,7 +578,7 @@ struct Engine : EngineBase {
     const size_t N = ps * NZ;
     learned_features_into(lfeat.p, false, re_tau);
     const long long ntiles = ((long long)N + 127) / 128;
-    const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, nsm);
+    const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, (long long)nsm * kInferCtasPerSm);
     MlpOutTau<T> out{ltau.p, (long long)N};
     launch(k_mlp_infer<MlpOutTau<T>>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, st, mlp,
            (const uint4*)lfeat.p, (long long)N, out, lpart.p, err.p);

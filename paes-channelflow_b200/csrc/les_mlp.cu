@@ -208,7 +208,7 @@ int les_mlp_forward(les_mlp* m, const void* feat, long long n, float* y, void* s
     check_samples(feat, y, n);
     cudaStream_t s = (cudaStream_t)stream;
     const long long ntiles = (n + 127) / 128;
-    const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, m->nsm);
+    const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, (long long)m->nsm * kInferCtasPerSm);
     launch(k_mlp_infer<MlpOutRaw>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, s, (const MlpDev*)m->dev,
            (const uint4*)feat, n, MlpOutRaw{y}, (double*)nullptr, m->err.p);
   });

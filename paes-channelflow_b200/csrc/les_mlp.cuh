@@ -116,6 +116,7 @@ __device__ __forceinline__ void issue_layer(uint32_t d, uint32_t a_s, uint32_t w
 // term summed per CTA into dissip_part[blockIdx.x] (when non-null).
 // ------------------------------------------------------------------------
 constexpr int kInferGroups = 4;
+constexpr int kInferCtasPerSm = 2;  // 2 x 256 tensor-memory columns, 2 x 87 KB shared memory
 constexpr size_t kInferSmem = sizeof(MlpDev) + (size_t)kInferGroups * 16384 + 256;
 
 // One group's view of its tile: shared-memory addresses of its activation
@@ -216,7 +217,7 @@ __device__ __forceinline__ void mlp_tile_failed(MlpGroup& G, int r, int* err) {
 }
 
 template <class Out>
-__global__ void __launch_bounds__(128 * kInferGroups, 1)
+__global__ void __launch_bounds__(128 * kInferGroups, kInferCtasPerSm)
 k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long long n, Out out,
             double* __restrict__ dissip_part, int* __restrict__ err) {
   constexpr int G = kInferGroups;
