@@ -93,6 +93,17 @@ int les_gpu_upload(les_handle* h, const void* u, const void* v, const void* w,
                    const void* e, const void* p, int real_bytes);
 int les_gpu_download(les_handle* h, void* u, void* v, void* w, void* e, void* p,
                      int real_bytes);
+/* Regridding (replaces the offline program redim.f90 plus the restart that
+ * reads its output): dst's state (u, v, w, e, p) becomes src's state moved
+ * onto dst's grid -- redim's linear z interpolation from src's levels
+ * (interpol, redim.f90:214-287), spectral truncation / zero padding in x
+ * and y (subroutine redim, redim.f90:292-327), e clamped to [1e-10, plane
+ * maximum] (redim.f90:276-277), then the restart's deal of u, v, w, e
+ * (les.F90:185-190) and w(nnz) = 0.  Both handles: same precision, device
+ * and domain lengths (xl, yl, zl), else LES_EINVAL; any nnx, nny, nnz
+ * each.  Synchronous; src is only read.  dst's tendencies are left as they
+ * are (a restart starts a new RK3 step). */
+int les_gpu_regrid(les_handle* dst, les_handle* src);
 /* The tendencies ru, rv, rw, re (storage module, modules.f90:25-26). */
 int les_gpu_upload_tendencies(les_handle* h, const void* ru, const void* rv,
                               const void* rw, const void* re, int real_bytes);

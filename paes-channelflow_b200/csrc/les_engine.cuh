@@ -22,6 +22,7 @@
 #include "../../include/les_gpu.h"
 #include "les_fused.cuh"
 #include "les_learned.cuh"
+#include "les_regrid.cuh"
 
 namespace les {
 
@@ -116,6 +117,23 @@ template <class T> struct DevBuf {
   }
 };
 
+// Device scratch of one call, freed when the call returns (also on errors).
+struct TmpDev {
+  std::vector<void*> p;
+  TmpDev() = default;
+  TmpDev(const TmpDev&) = delete;
+  TmpDev& operator=(const TmpDev&) = delete;
+  ~TmpDev() {
+    for (void* q : p) cudaFree(q);
+  }
+  template <class U> U* get(size_t n) {
+    void* q = nullptr;
+    LES_CUDA(cudaMalloc(&q, (n ? n : 1) * sizeof(U)));
+    p.push_back(q);
+    return (U*)q;
+  }
+};
+
 // Operator-level helpers on caller buffers (les_op_* entry points).
 template <class T>
 void op_expand(const T* in, T* out, int nx, int ny, int howmany, cudaStream_t s, cx<T>* t1, cx<T>* t2);
@@ -150,6 +168,8 @@ struct EngineBase {
   virtual void learned_status(int* used, double* dissipation) = 0;
   virtual void learned_features(double re_tau, float* feat) = 0;
   virtual void learn_filter(int fxy, int fz, int with_model, double* out) = 0;
+  // this state := the state of `src` regridded onto this grid (redim.f90)
+  virtual void regrid_from(EngineBase& src) = 0;
 };
 
 template <class T>
@@ -516,6 +536,64 @@ struct Engine : EngineBase {
     });
   }
   // raw (unnormalised) features of the current state, f32 [N][16]
+  // ---- regridding (redim.f90 on the device, then the restart's deal) ----
+  void regrid_from(EngineBase& other) override {
+    auto* sp = dynamic_cast<Engine<T>*>(&other);
+    if (!sp) throw std::invalid_argument("regrid: both handles must use the same precision");
+    if (sp == this) throw std::invalid_argument("regrid: source and destination are the same handle");
+    Engine<T>& s = *sp;
+    if (s.dev != dev) throw std::invalid_argument("regrid: both handles must be on the same device");
+    if (s.cfg.xl != cfg.xl || s.cfg.yl != cfg.yl || s.cfg.zl != cfg.zl)
+      throw std::invalid_argument("regrid: both grids must cover the same domain (xl, yl, zl)");
+    TmpDev tmp;
+    const std::vector<RegridLevel> h = regrid_table(s.NZ, NZ, cfg.zl);
+    RegridLevel* tab = tmp.get<RegridLevel>(NZ);
+    LES_CUDA(cudaMemcpyAsync(tab, h.data(), NZ * sizeof(RegridLevel), cudaMemcpyHostToDevice, st));
+    LES_CUDA(cudaStreamSynchronize(s.st));  // the source state is complete
+    const dim3 gs(cdiv(nm, 256), NZ);
+    auto spec = [&](const cx<T>* a, cx<T>* b, int mode) {
+      launch(k_regrid_spec<cx<T>, T>, gs, dim3(256), 0, st, a, b, (const RegridLevel*)tab, mode, s.KX, s.NY, KX, NY);
+    };
+    spec(s.uh.p, uh.p, kRegridCentre);
+    spec(s.vh.p, vh.p, kRegridCentre);
+    spec(s.wh.p, wh.p, kRegridFace);
+    launch(k_regrid_spec<cx<double>, double>, gs, dim3(256), 0, st, (const cx<double>*)s.ph.p, ph.p,
+           (const RegridLevel*)tab, (int)kRegridCentre, s.KX, s.NY, KX, NY);
+    LES_CUDA(cudaMemsetAsync(wh.p + nm * (NZ - 1), 0, nm * sizeof(cx<T>), st));  // w(nnz) = 0
+    for (auto pr : {std::make_pair(s.mu.p, mu.p), std::make_pair(s.mv.p, mv.p)})
+      launch(k_regrid_mean, dim3(cdiv(NZ, 128)), dim3(128), 0, st, (const double*)pr.first, pr.second,
+             (const RegridLevel*)tab, NZ);
+    launch(k_set_mean<T>, dim3(cdiv(NZ, 128)), dim3(128), 0, st, uh.p, (const double*)mu.p, nm, NZ);
+    launch(k_set_mean<T>, dim3(cdiv(NZ, 128)), dim3(128), 0, st, vh.p, (const double*)mv.p, nm, NZ);
+    // e: chunks of at most min(NZ_old, NZ_new) levels (the old grid's
+    // transform scratch holds NZ_old planes)
+    const int chunk = std::min(s.NZ, NZ);
+    T* ez = tmp.get<T>((size_t)chunk * s.ps);
+    cx<T>* es = tmp.get<cx<T>>((size_t)chunk * s.nm);
+    cx<T>* ed = tmp.get<cx<T>>((size_t)chunk * nm);
+    double* emax = tmp.get<double>(NZ);
+    for (int n0 = 0; n0 < NZ; n0 += chunk) {
+      const int cnt = std::min(chunk, NZ - n0);
+      launch(k_regrid_ez<T>, dim3(cdiv(s.ps, 256), cnt), dim3(256), 0, st, (const T*)(s.e.p + s.ps), ez,
+             (const RegridLevel*)tab, n0, s.ps);
+      launch(k_plane_max<T>, dim3(cnt), dim3(256), 0, st, (const T*)ez, s.ps, emax + n0);
+      LES_CUDA(cudaStreamSynchronize(st));
+      s.to_spectral(ez, es, cnt);  // on the source's stream, old grid
+      LES_CUDA(cudaStreamSynchronize(s.st));
+      launch(k_regrid_spec<cx<T>, T>, dim3(cdiv(nm, 256), cnt), dim3(256), 0, st, (const cx<T>*)es, ed,
+             (const RegridLevel*)nullptr, (int)kRegridCopy, s.KX, s.NY, KX, NY);
+      T* en = e.p + ps * (size_t)(n0 + 1);
+      to_physical(ed, en, cnt);
+      launch(k_regrid_eclamp<T>, dim3(cdiv(ps, 256), cnt), dim3(256), 0, st, en, (const double*)(emax + n0), ps);
+    }
+    // the restart's deal of e
+    to_spectral(e.p + ps, run.p, NZ);
+    to_physical(run.p, e.p + ps, NZ);
+    LES_CUDA(cudaMemsetAsync(run.p, 0, nm * NZ * sizeof(cx<T>), st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    phase = 0;
+  }
+
   void learned_features(double rt, float* feat) override {
     if (phase != 0) throw std::logic_error("learned_features inside a split comp1..comp2 sequence");
     learned_alloc();

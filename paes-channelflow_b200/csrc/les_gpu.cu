@@ -136,6 +136,9 @@ int guarded(les_handle* h, F&& fn) {
   } catch (CudaError& e) {
     h->err = e.what();
     rc = e.code;
+  } catch (std::invalid_argument& e) {
+    h->err = e.what();
+    rc = LES_EINVAL;
   } catch (std::logic_error& e) {
     h->err = e.what();
     rc = LES_ESTATE;
@@ -290,6 +293,14 @@ int les_gpu_upload(les_handle* h, const void* u, const void* v, const void* w, c
 int les_gpu_download(les_handle* h, void* u, void* v, void* w, void* e, void* p, int real_bytes) {
   if (check_rb(real_bytes)) return LES_EINVAL;
   return guarded(h, [&] { h->eng->download(u, v, w, e, p, real_bytes); });
+}
+int les_gpu_regrid(les_handle* dst, les_handle* src) {
+  if (!dst || !src) return LES_EINVAL;
+  if (dst == src) {
+    dst->err = "les_gpu_regrid: source and destination are the same handle";
+    return LES_EINVAL;
+  }
+  return guarded(dst, [&] { dst->eng->regrid_from(*src->eng); });
 }
 int les_gpu_upload_tendencies(les_handle* h, const void* ru, const void* rv, const void* rw, const void* re,
                               int real_bytes) {

@@ -38,6 +38,11 @@ module les_gpu
        type(c_ptr), value :: h, u, v, w, e, p
        integer(c_int), value :: rb
      end function
+     ! redim.f90 on the device: dst's state := src's state on dst's grid
+     integer(c_int) function les_gpu_regrid(dst, src) bind(C, name="les_gpu_regrid")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: dst, src
+     end function
      integer(c_int) function les_gpu_lower(h) bind(C, name="les_gpu_lower")
        import :: c_ptr, c_int
        type(c_ptr), value :: h

@@ -136,6 +136,7 @@ def lib():
         "les_gpu_write_field": (I, [H, ctypes.c_char_p, D, I, I]),
         "les_gpu_field_wait": (I, [H]),
         "les_gpu_read_field": (I, [H, ctypes.c_char_p, I, ctypes.POINTER(D)]),
+        "les_gpu_regrid": (I, [H, H]),
         "les_gpu_field_header": (I, [ctypes.c_char_p, I, ctypes.POINTER(I), ctypes.POINTER(D)]),
         "les_gpu_learned_features": (I, [H, D, VP]),
     }
@@ -322,6 +323,11 @@ class LesGpu:
         t = ctypes.c_double()
         self._check(lib().les_gpu_read_field(self.h, os.fsencode(path), real_bytes, ctypes.byref(t)))
         return t.value
+
+    def regrid_from(self, src):
+        """This handle's state := src's state moved onto this grid (redim.f90
+        followed by the restart's deal); see les_gpu_regrid."""
+        self._check(lib().les_gpu_regrid(self.h, src.h))
 
     def sync(self, timeout_s=60.0):
         self._check(lib().les_gpu_sync(self.h, timeout_s))
@@ -543,6 +549,26 @@ def to_target(t):
     o = torch.zeros((t.shape[0], 8), dtype=torch.float32)
     o[:, :MLP_NOUT] = t
     return o.cuda()
+
+
+def regrid_field(path_in, path_out, nnx, nny, nnz, real_bytes=8, precision=PREC_FP64, device=0):
+    """The reference's redim program on restart files: read path_in (any
+    grid), regrid its state onto nnx x nny x nnz on the GPU and write
+    path_out with the input's time, lengths, dt and z0."""
+    dims, hdr = field_header(path_in, real_bytes)
+    cfgs = []
+    for n in (dims, (nnx, nny, nnz)):
+        c = channel_config(*n, dt=hdr["dt"], precision=precision, device=device)
+        c.xl, c.yl, c.zl, c.z0 = hdr["xl"], hdr["yl"], hdr["zl"], hdr["z0"]
+        cfgs.append(c)
+    src, dst = LesGpu(cfgs[0]), LesGpu(cfgs[1])
+    try:
+        t = src.read_field(path_in, real_bytes)
+        dst.regrid_from(src)
+        dst.write_field(path_out, time=t, real_bytes=real_bytes)
+    finally:
+        dst.close()
+        src.close()
 
 
 def field_header(path, real_bytes=8):

@@ -134,6 +134,26 @@ def test_c1_ten_steps_fp64(gpu_lib, product):
     np.testing.assert_allclose(sg[:4], so[:4], rtol=1e-9, atol=1e-15)
 
 
+@pytest.mark.parametrize("n", [256, 384, 512])
+def test_fused_row_plans_at_production_widths(gpu_lib, product, n):
+    """The fused row kernel's transform plans of the production grids (padded
+    rows 384 and 576: two-pass with 24-point register DFTs; 768: three-pass
+    Stockham) against the oracle, one stage in each precision (nz = 4 keeps
+    the oracle to seconds)."""
+    o, g, _ = make_pair(product, n, n, 4, amp=0.3)
+    o.stage(0, 1, 1)
+    g.stage(0, True, 1)
+    compare(o, g, 1e-11, 1e-9, "fp64 %d" % n)
+    o, g, _ = make_pair(product, n, n, 4, precision=4, amp=0.3)
+    o.stage(0, 1, 1)
+    g.stage(0, True, 1)
+    fo, fg = o.get_fields(), g.download()
+    vscale = np.abs(fo["u"]).max()
+    for k in "uvw":
+        assert relerr(fg[k], fo[k], vscale) < 2e-5, (n, k)
+    assert relerr(fg["e"], fo["e"]) < 2e-5, n
+
+
 def test_mixed_precision_envelope(gpu_lib, product):
     o, g, f = make_pair(product, 64, 64, 32, precision=4, amp=0.1)
     for it in range(3):
