@@ -382,7 +382,7 @@ def main():
     ab = algorithmic_bytes(kname, NX, NY, NZ, 4)
     achieved = ab / (kms / 1e3) / 1e9 if ab else None
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic_c5.txt")
+    tfile = os.path.join(ROOT, "profiles", "traffic_k_row_fused_512x512x256.txt")
     if os.path.exists(tfile):
         for ln in open(tfile):
             f = ln.split()

@@ -735,7 +735,7 @@ struct Engine : EngineBase {
     nch = (int)cdiv(NZ, fa.zchunk);
     with_small(NX, [&](auto cn) {
       constexpr int N = decltype(cn)::value;
-      launch(k_row_fused<T, N>, dim3(MY, nch), dim3(FusedCfg<N>::THREADS), FusedCfg<N>::template smem<T>(), st, fa,
+      launch(k_row_fused<T, N>, dim3(MY, nch), dim3(FusedCfg<N>::template threads<T>()), FusedCfg<N>::template smem<T>(), st, fa,
              a, tw);
     });
   }

@@ -6,15 +6,17 @@
 // The CTA walks up its z chunk keeping a window of physical rows in shared
 // memory (levels z-1, z, z+1 of U, V, W, E, packed as complex rows U+iV and
 // W+iE), exactly the sliding window of comp1.f90:91-121 / 179-184 but along
-// one row of the padded plane.  Six warps each own one transform per phase:
+// one row of the padded plane.  Six teams (one warp each) each own one
+// transform per phase:
 //   phase I   (inverse)  w0: U+iV (z+1)   w1: W+iE (z+1)   w2: UX+iVX (z)
 //                        w3: UY+iVY (z)   w4: WX+iWY (z)   w5: EX+iEY (le)
 //   phase II  (pointwise, all threads) the eleven flux rows of k_flux
 //   phase III (forward)  w0: A+iPu  w1: B+iPv  w2: C+iG  w3: D+iPw
 //                        w4: F+iPe  w5: H
 // Transforms are warp-synchronous four-step FFTs (lanes = N2 in pass A,
-// N1 in pass B, __syncwarp between passes); block barriers only separate
-// the three phases.
+// N1 in pass B, __syncwarp between passes) or, for rows whose second
+// factor exceeds 24 (768), three Stockham passes synchronised by the team's
+// named barrier; block barriers only separate the three phases.
 #pragma once
 #include "les_kernels.cuh"
 
@@ -170,10 +172,16 @@ template <int N, class T> struct FusedPlan {
   static constexpr bool three = (Split<N>::N2 > 24);
   static constexpr int BUF = three ? N : smem_fft_elems<N, false>(1);
 };
-template <int N, int S, bool IN_SMEM, class T, class LoadF>
-__device__ __forceinline__ void fused_fft(cx<T>* buf, const cx<T>* twn, LoadF load, int lane) {
-  if constexpr (FusedPlan<N, T>::three) team_fft<N, S, IN_SMEM, 32, T>(buf, twn, load, lane, 0);
-  else warp_fft<N, S, IN_SMEM, T>(buf, twn, load);
+// One transform by a team of TEAM threads (tl = index in the team, bar = the
+// team's named barrier; the two-pass warp form needs TEAM = 32).
+template <int N, int S, bool IN_SMEM, int TEAM, class T, class LoadF>
+__device__ __forceinline__ void fused_fft(cx<T>* buf, const cx<T>* twn, LoadF load, int tl, int bar) {
+  if constexpr (FusedPlan<N, T>::three) {
+    team_fft<N, S, IN_SMEM, TEAM, T>(buf, twn, load, tl, bar);
+  } else {
+    static_assert(TEAM == 32, "the two-pass transform is warp-synchronous");
+    warp_fft<N, S, IN_SMEM, T>(buf, twn, load);
+  }
 }
 
 struct FusedArgs {
@@ -195,8 +203,11 @@ struct FusedArgs {
 template <int NSX> struct FusedCfg {
   static constexpr int MX = 3 * NSX / 2;
   static constexpr int NBUF = 11;  // 6 level slots (3 levels x 2), 4 work buffers, 1 carried tuw/tvw
-  static constexpr int TEAM = 32;  // one warp per transform
-  static constexpr int THREADS = 6 * TEAM;
+  // threads per transform: one warp.  (Two warps for the FP64 768-point
+  // plan double the resident warps but cap the 384-thread block at 168
+  // registers, which spills; on B200 that ran 9% slower.)
+  template <class T> static constexpr int team() { return 32; }
+  template <class T> static constexpr int threads() { return 6 * team<T>(); }
   template <class T> static constexpr int buf() { return FusedPlan<MX, T>::BUF; }
   // buffers + the twiddle table of length MX staged in shared memory
   template <class T> static constexpr size_t smem() {
@@ -205,12 +216,12 @@ template <int NSX> struct FusedCfg {
 };
 
 template <class T, int NSX>
-__global__ void __launch_bounds__(192, (sizeof(T) == 4) ? 2 : 1)
+__global__ void __launch_bounds__(FusedCfg<NSX>::template threads<T>(), (sizeof(T) == 4) ? 2 : 1)
 k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   constexpr int MX = 3 * NSX / 2;
   constexpr int KX = NSX / 2;
   constexpr int BUF = FusedCfg<NSX>::template buf<T>();
-  constexpr int TEAM = FusedCfg<NSX>::TEAM;
+  constexpr int TEAM = FusedCfg<NSX>::template team<T>();
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
   // twiddles staged once per CTA in the layout each transform reads with
@@ -241,7 +252,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   const int z0 = blockIdx.y * f.zchunk + 1;
   const int z1 = min(z0 + f.zchunk - 1, NZ);
   if (z0 > NZ) return;
-  // team w (threads [64w, 64w+64)) owns transform w of every phase
+  // team w (threads [TEAM w, TEAM (w+1))) owns transform w of every phase
   const int warp = threadIdx.x / TEAM, lane = threadIdx.x % TEAM;
   const int bar = 1 + warp;
   auto S = [](int q) { return Swz<T, MX>::f(q); };  // swizzled position of element q
@@ -273,7 +284,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   };
   // inverse transform of one (A, B) pair into buf (by the calling team)
   auto inv = [&](cx<T>* buf, const cx<T>* A, bool ma, const cx<T>* B, bool mb) {
-    fused_fft<MX, +1, false, T>(buf, tws, [&](int n) { return c2r_load(A, ma, B, mb, n); }, lane);
+    fused_fft<MX, +1, false, TEAM, T>(buf, tws, [&](int n) { return c2r_load(A, ma, B, mb, n); }, lane, bar);
   };
   auto clipE = [&](cx<T>* we) {
     for (int x = lane; x < MX; x += TEAM) we[S(x)].y = tmax(we[S(x)].y, emin);
@@ -445,7 +456,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
     // ---- phase III: forward transforms, -d/dx, truncation to kx < nx/2 ----
     if (!(top && warp >= 3)) {
       cx<T>* buf = work[warp];
-      fused_fft<MX, -1, true, T>(buf, tws, NoLoad{}, lane);
+      fused_fft<MX, -1, true, TEAM, T>(buf, tws, NoLoad{}, lane, bar);
       const size_t orow = ((size_t)(z - 1) * MY + y) * KX;
       auto O = [&](int j) { return reinterpret_cast<cx<T>*>(f.out.p[j]) + orow; };
       for (int k = lane; k < KX; k += TEAM) {
