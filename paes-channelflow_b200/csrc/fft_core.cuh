@@ -349,14 +349,14 @@ __device__ __forceinline__ void smem_fft(int ntrans, cx<T>* sm, const cx<T>* __r
 //   natural layout: rows  sm[t*N + n];  cols (COLS) sm[n*ntrans + t]
 // Requires blockDim.x >= ntrans*N2 and smem_fft_elems<N, COLS>(ntrans)
 // elements; every thread of the block must call it.  Ends with a
-// __syncthreads() when OUT_SMEM.
+// __syncthreads() when OUT_SMEM.  fft_core_tab takes the length-N twiddle
+// table itself (e.g. staged in shared memory by stage_twiddles); fft_core
+// reads it from the global table.
 template <int N, int S, bool COLS, bool IN_SMEM, bool OUT_SMEM, class T, class LoadF, class StoreF>
-__device__ __forceinline__ void fft_core(int ntrans, cx<T>* sm, const cx<T>* __restrict__ tw, LoadF load,
-                                         StoreF store) {
+__device__ __forceinline__ void fft_core_tab(int ntrans, cx<T>* sm, const cx<T>* twn, LoadF load, StoreF store) {
   constexpr int N1 = Split<N>::N1;
   constexpr int N2 = Split<N>::N2;
   constexpr int LD = N2 + 1;
-  const cx<T>* twn = tw + tw_off(N);
   const int it = threadIdx.x;
   {
     const bool active = it < ntrans * N2;
@@ -413,6 +413,20 @@ __device__ __forceinline__ void fft_core(int ntrans, cx<T>* sm, const cx<T>* __r
     }
     if (OUT_SMEM) __syncthreads();
   }
+}
+template <int N, int S, bool COLS, bool IN_SMEM, bool OUT_SMEM, class T, class LoadF, class StoreF>
+__device__ __forceinline__ void fft_core(int ntrans, cx<T>* sm, const cx<T>* __restrict__ tw, LoadF load,
+                                         StoreF store) {
+  fft_core_tab<N, S, COLS, IN_SMEM, OUT_SMEM, T>(ntrans, sm, tw + tw_off(N), load, store);
+}
+// Copy of the length-N twiddle table into shared memory `dst` (N entries),
+// by the whole block; ends with a barrier.
+template <int N, class T>
+__device__ __forceinline__ const cx<T>* stage_twiddles(cx<T>* dst, const cx<T>* __restrict__ tw) {
+  const cx<T>* g = tw + tw_off(N);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) dst[i] = g[i];
+  __syncthreads();
+  return dst;
 }
 struct NoLoad {
   __device__ int operator()(int, int) const { return 0; }

@@ -777,7 +777,10 @@ k_y_forward(Ptr8 X, Ptr8 rnew, int KX, int NZ, T ky0, T scale, const cx<T>* __re
   const int kx0 = blockIdx.x * C::TC;
   const cx<T>* X1 = (const cx<T>*)X.p[2 * f] + (size_t)(z - 1) * M * KX;
   const cx<T>* X2 = (const cx<T>*)X.p[2 * f + 1] + (size_t)(z - 1) * M * KX;
-  fft_core<M, -1, true, false, true>(TC2, sm, tw, [&](int t, int n) {
+  // the twiddles of the M-point transform staged in shared memory (measured
+  // faster here than reading them through L1)
+  const cx<T>* tws = stage_twiddles<M>(sm3 + C::TC * NS, tw);
+  fft_core_tab<M, -1, true, false, true>(TC2, sm, tws, [&](int t, int n) {
     int tt = t % C::TC, kx = kx0 + tt;
     const cx<T>* src = (t < C::TC) ? X1 : X2;
     return (kx < KX) ? src[(size_t)n * KX + kx] : zero_cx<T>();
