@@ -70,9 +70,10 @@ template <int NX> struct LgxCfg {
   static constexpr int N1 = Split<NX>::N1, N2 = Split<NX>::N2, M12 = N1 > N2 ? N1 : N2;
   static constexpr int RB = (256 / (5 * M12)) > 0 ? (256 / (5 * M12)) : 1;
   static constexpr int THREADS = 5 * RB * M12;
-  template <class T> static constexpr size_t smem() {
-    return (size_t)smem_fft_elems<NX, false>(5 * RB) * sizeof(cx<T>);
-  }
+  static constexpr int BUF = smem_fft_elems<NX, false>(5 * RB);
+  // transform buffer + the staged spectra (direct and mirrored combination
+  // of each of the 5*RB transforms at kx < NX/2)
+  template <class T> static constexpr size_t smem() { return (size_t)(BUF + 10 * RB * (NX / 2)) * sizeof(cx<T>); }
 };
 
 // Gradients and features at the cell centres of RB rows (one level, RB
@@ -92,36 +93,46 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
   const size_t r0 = (size_t)blockIdx.x * RB;
   // row of field f at level k (1..NZ) and y
   auto rowp = [&](int f, int k, int y) -> const cx<T>* { return gy + (size_t)f * plane + ((size_t)(k - 1) * NY + y) * KX; };
-  fft_core<NX, +1, false, false, true>(5 * RB, sm, tw, [&](int t, int n) -> cx<T> {
+  // Stage 1: the spectral combinations a + i b of the five transforms of
+  // each row at kx = 0..KX-1, loaded once (coalesced along kx), kept as the
+  // direct value (position kx) and the conjugate-symmetric one (NX - kx).
+  cx<T>* zd = sm + L::BUF;             // [5*RB][KX]
+  cx<T>* zm = zd + (size_t)5 * RB * KX;  // [5*RB][KX]
+  for (int i = threadIdx.x; i < 5 * RB * KX; i += blockDim.x) {
+    const int t = i / KX, k = i - t * KX;
     const int rr = t / 5, j = t - 5 * rr;
     const size_t row = r0 + rr;
-    if (row >= R) return zero_cx<T>();
-    int k = n;
-    bool mir = false;
-    if (k >= KX) {
-      if (NX - k < KX) { k = NX - k; mir = true; }
-      else k = -1;
+    cx<T> d = zero_cx<T>(), m = zero_cx<T>();
+    if (row < R) {
+      const int z = (int)(row / NY) + 1, y = (int)(row - (size_t)(z - 1) * NY);
+      const T xk = kx0 * (T)k;
+      auto wl = [&](int f, int kk) -> cx<T> { return (kk >= 1 && kk <= NZ - 1) ? rowp(f, kk, y)[k] : zero_cx<T>(); };
+      auto vz = [&](int f) -> cx<T> {
+        if (z == 1) return (rowp(f, 2, y)[k] - rowp(f, 1, y)[k]) * dzm;
+        if (z == NZ) return (rowp(f, NZ, y)[k] - rowp(f, NZ - 1, y)[k]) * dzm;
+        return (rowp(f, z + 1, y)[k] - rowp(f, z - 1, y)[k]) * ((T)0.5 * dzm);
+      };
+      cx<T> a, b;
+      switch (j) {
+        case 0: a = mul_i(rowp(0, z, y)[k]) * xk; b = mul_i(rowp(2, z, y)[k]) * xk; break;      // ux, vx
+        case 1: a = mul_i(wl(4, z) + wl(4, z - 1)) * ((T)0.5 * xk); b = rowp(1, z, y)[k]; break; // wx, uy
+        case 2: a = rowp(3, z, y)[k]; b = (wl(5, z) + wl(5, z - 1)) * (T)0.5; break;            // vy, wy
+        case 3: a = vz(0); b = vz(2); break;                                                    // uz, vz
+        default: a = (wl(4, z) - wl(4, z - 1)) * dzm; b = zero_cx<T>(); break;                  // wz
+      }
+      if (k == 0) { a.y = 0; b.y = 0; }
+      d = mk(a.x - b.y, a.y + b.x);  // a + i b
+      m = mk(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
     }
-    if (k < 0) return zero_cx<T>();
-    const int z = (int)(row / NY) + 1, y = (int)(row - (size_t)(z - 1) * NY);
-    const T xk = kx0 * (T)k;
-    auto wl = [&](int f, int kk) -> cx<T> { return (kk >= 1 && kk <= NZ - 1) ? rowp(f, kk, y)[k] : zero_cx<T>(); };
-    auto vz = [&](int f) -> cx<T> {
-      if (z == 1) return (rowp(f, 2, y)[k] - rowp(f, 1, y)[k]) * dzm;
-      if (z == NZ) return (rowp(f, NZ, y)[k] - rowp(f, NZ - 1, y)[k]) * dzm;
-      return (rowp(f, z + 1, y)[k] - rowp(f, z - 1, y)[k]) * ((T)0.5 * dzm);
-    };
-    cx<T> a, b;
-    switch (j) {
-      case 0: a = mul_i(rowp(0, z, y)[k]) * xk; b = mul_i(rowp(2, z, y)[k]) * xk; break;      // ux, vx
-      case 1: a = mul_i(wl(4, z) + wl(4, z - 1)) * ((T)0.5 * xk); b = rowp(1, z, y)[k]; break; // wx, uy
-      case 2: a = rowp(3, z, y)[k]; b = (wl(5, z) + wl(5, z - 1)) * (T)0.5; break;            // vy, wy
-      case 3: a = vz(0); b = vz(2); break;                                                    // uz, vz
-      default: a = (wl(4, z) - wl(4, z - 1)) * dzm; b = zero_cx<T>(); break;                  // wz
-    }
-    if (k == 0) { a.y = 0; b.y = 0; }
-    if (mir) { a = conj(a); b = conj(b); }
-    return mk(a.x - b.y, a.y + b.x);
+    zd[i] = d;
+    zm[i] = m;
+  }
+  __syncthreads();
+  // Stage 2: the inverse transforms from the staged spectra
+  fft_core<NX, +1, false, false, true>(5 * RB, sm, tw, [&](int t, int n) -> cx<T> {
+    if (n < KX) return zd[(size_t)t * KX + n];
+    if (NX - n < KX) return zm[(size_t)t * KX + (NX - n)];
+    return zero_cx<T>();
   }, NoStore{});
   for (int i = threadIdx.x; i < RB * NX; i += blockDim.x) {
     const int rr = i / NX, x = i - rr * NX;
