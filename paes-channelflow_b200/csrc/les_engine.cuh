@@ -519,7 +519,7 @@ struct Engine : EngineBase {
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = ColCfg<NN, T>;
-      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC), NZ, 6), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
+      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC / 2), NZ, 3), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
              (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)ky0, tw);
     });
     const T zpl = (T)(rt / (cfg.zl / 2.0));

@@ -39,28 +39,32 @@
 
 namespace les {
 
-// y-inverse rows gy[f][z][y][kx], f = 0..5: U, UY, V, VY, W, WY
+// y-inverse rows gy[f][z][y][kx], f = 0..5: U, UY, V, VY, W, WY.  A block
+// takes H = TC/2 columns of one component (blockIdx.z: u, v, w) at one
+// level and runs 2H transforms: t < H the field, t >= H its y derivative,
+// so each spectral value is read once.
 template <class T, int N>
 __global__ void __launch_bounds__(ColCfg<N, T>::THREADS)
 k_lgrad_y(const cx<T>* __restrict__ uh, const cx<T>* __restrict__ vh, const cx<T>* __restrict__ wh,
           cx<T>* __restrict__ gy, int KX, int NZ, T ky0, const cx<T>* __restrict__ tw) {
   using C = ColCfg<N, T>;
+  constexpr int H = C::TC / 2;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
   const int z = blockIdx.y + 1;
-  const int f = blockIdx.z;
-  const int c0 = blockIdx.x * C::TC;
+  const int c = blockIdx.z;
+  const int c0 = blockIdx.x * H;
   const size_t nm = (size_t)N * KX;
-  const cx<T>* src = (f < 2 ? uh : (f < 4 ? vh : wh)) + (size_t)(z - 1) * nm;
-  const bool zero = (f >= 4 && z == NZ);  // w(nnz) = 0
-  const bool dy = (f & 1);
-  fft_core<N, +1, true, false, false>(C::TC, sm, tw, [&](int t, int n) -> cx<T> {
-    const int kx = c0 + t;
+  const cx<T>* src = (c == 0 ? uh : (c == 1 ? vh : wh)) + (size_t)(z - 1) * nm;
+  const bool zero = (c == 2 && z == NZ);  // w(nnz) = 0
+  fft_core<N, +1, true, false, false>(2 * H, sm, tw, [&](int t, int n) -> cx<T> {
+    const int kx = c0 + (t < H ? t : t - H);
     if (kx >= KX || n == N / 2 || zero) return zero_cx<T>();
     const cx<T> v = src[(size_t)n * KX + kx];
-    return dy ? mul_i(v) * (ky0 * (T)signed_k(n, N)) : v;
+    return t >= H ? mul_i(v) * (ky0 * (T)signed_k(n, N)) : v;
   }, [&](int t, int k, cx<T> v) {
-    const int kx = c0 + t;
+    const int kx = c0 + (t < H ? t : t - H);
+    const int f = 2 * c + (t < H ? 0 : 1);
     if (kx < KX) gy[((size_t)f * NZ + (z - 1)) * nm + (size_t)k * KX + kx] = v;
   });
 }
