@@ -47,6 +47,8 @@ NX = NY = 512
 NZ = 256
 RE_TAU = 590.0
 SLAB_NZ = 4
+# levels (1-based) of the stated x-spectrum errors: nearest z+ = 15 and z+ = 100
+SPEC_LEVELS = tuple(int(round(zp / (2.0 / NZ * RE_TAU) + 0.5)) for zp in (15.0, 100.0))
 METRIC = "RK3 Mpoint-steps/s"
 
 
@@ -217,6 +219,8 @@ def run_form(P, precision, steps, warmup, dev, want_profile, imodel=3, mlp=None)
     out["utau"] = float(sc[0])
     out["divz_max"] = float(np.max(mb[2]))
     out["meanbuf"] = mb
+    # 1D x-spectra of u and w at the levels nearest z+ = 15 and 100
+    out["spectra"] = {(f, iz): g.spectra(f, iz)[0] for f in (0, 2) for iz in SPEC_LEVELS}
     if mlp is not None:
         out["learned_status"] = g.learned_status()
     out["handle"] = g
@@ -264,14 +268,38 @@ def barrier():
         dist.barrier()
 
 
+def init_dist(backend, timeout_s=120):
+    """One process group over all ranks (env:// rendezvous: MASTER_ADDR,
+    MASTER_PORT, RANK, WORLD_SIZE); a short timeout so that ranks waiting for
+    a rank that died end with an error."""
+    global _pg
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    _pg = dist.group.WORLD
+
+
 def max_over_ranks(x):
     if _pg is None:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(points_per_rank, steps, ms_local):
+    """Whole-job rate of independent replicas (one per rank): the points of
+    all ranks times steps over the max-over-ranks time, in Mpoint-steps/s;
+    returns (rate, max ms)."""
+    world = 1
+    if _pg is not None:
+        import torch.distributed as dist
+        world = dist.get_world_size()
+    ms = max_over_ranks(ms_local)
+    return world * points_per_rank * steps / (ms / 1e3) / 1e6, ms
 
 
 def cpu_baseline(steps=1, threads=None):
@@ -291,7 +319,6 @@ def cpu_baseline(steps=1, threads=None):
 
 
 def main():
-    global _pg
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -325,11 +352,8 @@ def main():
 
     import torch
     if world > 1:
-        import datetime
-        import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        _pg = dist.group.WORLD
+        init_dist("nccl")
     dev = local_rank if world > 1 else 0
     torch.cuda.set_device(dev)
     P = load_product()
@@ -350,24 +374,26 @@ def main():
     mlp.close()
 
     pts = NX * NY * NZ
-    ms64 = max_over_ranks(r64["ms"])
-    ms32 = max_over_ranks(r32["ms"])
-    msl = max_over_ranks(rl["ms"])
-    e2e_s = max_over_ranks(e2e_s)
-    fp64 = world * pts * args.steps / (ms64 / 1e3) / 1e6
-    mixed = world * pts * args.steps / (ms32 / 1e3) / 1e6
-    value = world * pts * args.steps / (msl / 1e3) / 1e6
-    e2e = world * pts * args.steps / e2e_s / 1e6
+    fp64, ms64 = replica_rate(pts, args.steps, r64["ms"])
+    mixed, ms32 = replica_rate(pts, args.steps, r32["ms"])
+    value, msl = replica_rate(pts, args.steps, rl["ms"])
+    e2e, _ = replica_rate(pts, args.steps, 1e3 * e2e_s)
 
     # stated errors of the learned mixed (and mixed Deardorff) form against fp64
     def errors(r):
         a, b = r["meanbuf"], r64["meanbuf"]
         ub = float(np.mean(b[3]))
         rms = lambda m: np.sqrt(np.maximum(m[6], 0))
+        spec = {}
+        for (f, iz), sa in r["spectra"].items():
+            sb = r64["spectra"][(f, iz)]
+            key = "spectrum_%s_zplus%d_max_rel_err" % ("uw"[f // 2], round((iz - 0.5) * 2.0 / NZ * RE_TAU))
+            # over the resolved band, relative to each wavenumber's FP64 energy
+            spec[key] = float(np.max(np.abs(sa[1:NX // 3] - sb[1:NX // 3]) / np.maximum(sb[1:NX // 3], 1e-300)))
         return {"mean_u_max_err_over_ub": float(np.abs(a[3] - b[3]).max() / ub),
                 "uw_max_err_over_max": float(np.abs(a[9] - b[9]).max() / max(np.abs(b[9]).max(), 1e-300)),
                 "u_rms_max_err_over_max": float(np.abs(rms(a) - rms(b)).max() / max(rms(b).max(), 1e-300)),
-                "divz_max": float(np.max(a[2])), "divz_max_fp64": float(np.max(b[2])),
+                "divz_max": float(np.max(a[2])), "divz_max_fp64": float(np.max(b[2])), **spec,
                 "after_steps": args.warmup + args.steps}
 
     # roofline of the dominant kernel (per-kernel CUDA events on the handle's stream)

@@ -165,11 +165,12 @@ template <int N> __device__ __forceinline__ int stockham_twiddle_exp(int i) {
 }
 
 // Transform used by the fused kernel for a length: the two-pass warp form
-// unless its N2-point register DFT is longer than 24 (768 = 24 x 32), then
-// the three-pass Stockham form (radices <= 12, no register spills in either
-// precision).
+// unless its N2-point register DFT has 24 points or more (288, 384, 576,
+// 768), then the three-pass Stockham form (radices <= 12): the 24- and
+// 32-point register DFTs spill, and on B200 the three passes ran 6-31%
+// faster at 288-576.
 template <int N, class T> struct FusedPlan {
-  static constexpr bool three = (Split<N>::N2 > 24);
+  static constexpr bool three = (Split<N>::N2 >= 24);
   static constexpr int BUF = three ? N : smem_fft_elems<N, false>(1);
 };
 // One transform by a team of TEAM threads (tl = index in the team, bar = the

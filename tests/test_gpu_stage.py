@@ -134,12 +134,12 @@ def test_c1_ten_steps_fp64(gpu_lib, product):
     np.testing.assert_allclose(sg[:4], so[:4], rtol=1e-9, atol=1e-15)
 
 
-@pytest.mark.parametrize("n", [256, 384, 512])
+@pytest.mark.parametrize("n", [192, 256, 384, 512])
 def test_fused_row_plans_at_production_widths(gpu_lib, product, n):
-    """The fused row kernel's transform plans of the production grids (padded
-    rows 384 and 576: two-pass with 24-point register DFTs; 768: three-pass
-    Stockham) against the oracle, one stage in each precision (nz = 4 keeps
-    the oracle to seconds)."""
+    """The fused row kernel's three-pass Stockham plans of the production
+    grids (padded rows 288, 384, 576 and 768) against the oracle, one stage
+    in each precision (nz = 4 keeps the oracle to seconds); the stage tests
+    above cover the two-pass plans of the small grids."""
     o, g, _ = make_pair(product, n, n, 4, amp=0.3)
     o.stage(0, 1, 1)
     g.stage(0, True, 1)
