@@ -223,6 +223,7 @@ def run_form(P, precision, steps, warmup, dev, want_profile, imodel=3, mlp=None)
     out["spectra"] = {(f, iz): g.spectra(f, iz)[0] for f in (0, 2) for iz in SPEC_LEVELS}
     if mlp is not None:
         out["learned_status"] = g.learned_status()
+        out["learned_deardorff"] = g.learned_deardorff()
     out["handle"] = g
     return out
 
@@ -436,7 +437,8 @@ def main():
                   "fp64_ms_per_step": ms64 / args.steps, "mixed_ms_per_step": ms32 / args.steps,
                   "learned_mixed_ms_per_step": msl / args.steps,
                   "learned_used_last_stage": rl["learned_status"][0],
-                  "learned_dissipation_last_stage": rl["learned_status"][1]},
+                  "learned_dissipation_last_stage": rl["learned_status"][1],
+                  "deardorff_dissipation_last_stage": rl["learned_deardorff"]},
         "errors": {"learned_mixed_vs_fp64": errors(rl), "mixed_vs_fp64": errors(r32)},
         "e2e": {"value": e2e, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": rl["launches"],

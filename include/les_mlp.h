@@ -79,6 +79,19 @@ int les_gpu_set_mlp(les_handle* h, les_mlp* m, double re_tau);
  * dissipation -<tau_ij S_ij> of the network's stresses. */
 int les_gpu_learned_status(les_handle* h, int* used, double* dissipation);
 
+/* The fallback test of each stage: the network is used when its mean
+ * dissipation is >= 0 (the spec'd test) and, with ratio > 0, within a factor
+ * ratio of the Deardorff model's mean dissipation 2 <nu_t S_ij S_ij> on the
+ * same state (nu_t = min(0.1 Delta sqrt(e), xkmax) + nu, e at the cell
+ * centre).  The second test keeps a network out of states it was not
+ * trained for (a network trained on one grid imposes that grid's stress
+ * levels on another).  Default ratio 4; ratio <= 0 disables it.  Drops the
+ * handle's captured step graphs. */
+int les_gpu_set_learned_guard(les_handle* h, double ratio);
+/* After a synchronising call: the Deardorff mean dissipation of the last
+ * learned stage (the reference value of the second test). */
+int les_gpu_learned_deardorff(les_handle* h, double* dissipation);
+
 /* Training data (synchronous; out pointers are device memory).
  *
  * les_gpu_learn_filter: explicit filter of the handle's current state onto

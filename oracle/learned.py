@@ -110,6 +110,29 @@ def dissipation(g, tau):
     return float(d.mean())
 
 
+def deardorff_dissipation(g, e, dsl, xkmax, nu=0.0):
+    """Mean of 2 nu_t S_ij S_ij over all cell centres, nu_t = min(0.1 dsl
+    sqrt(e_c), xkmax) + nu with e_c = (e(k-1) + e(k)) / 2 and e(0) read as
+    e(1); e (nz, ny, nx) on the w-levels 1..nz."""
+    s11, s22, s33 = g[0], g[4], g[8]
+    s12, s13, s23 = 0.5 * (g[3] + g[1]), 0.5 * (g[6] + g[2]), 0.5 * (g[7] + g[5])
+    em = np.concatenate([e[:1], e[:-1]], axis=0)
+    ec = 0.5 * (em + e)
+    nut = np.minimum(0.1 * dsl * np.sqrt(np.maximum(ec, 0.0)), xkmax) + nu
+    ss = s11 ** 2 + s22 ** 2 + s33 ** 2 + 2 * (s12 ** 2 + s13 ** 2 + s23 ** 2)
+    return float((2 * nut * ss).mean())
+
+
+def network_used(dis, dis_d, guard):
+    """The stage's fallback rule: the network's mean dissipation must be
+    >= 0 and, with guard > 0, within a factor guard of Deardorff's."""
+    if not dis >= 0:
+        return 0
+    if guard > 0 and not (dis_d > 0 and dis <= guard * dis_d and guard * dis >= dis_d):
+        return 0
+    return 1
+
+
 def network_viscosity(g, tau, xkmax):
     """Face values (index j = w-level j) of the network's effective
     viscosity: per level -sum(tau13 uz + tau23 vz) / sum(uz^2 + vz^2)

@@ -347,6 +347,11 @@ struct Les {
   double re_tau = 0.0;
   int learned_used = 0;
   double learned_dissip = 0.0;
+  // second fallback test: the network's mean dissipation must lie within a
+  // factor `learned_guard` of the Deardorff model's on the same state
+  // (learned_guard <= 0: only the sign test)
+  double learned_guard = 4.0;
+  double learned_dissip_d = 0.0;
   T sgs_mom = (T)1;  // weight of the interior momentum stresses of compsgs1
   Levels<T> lru, lrv, lrw;
 
@@ -759,8 +764,11 @@ struct Les {
   //   wz = (w(k) - w(k-1))/dz; uz, vz = centred (u(k+1) - u(k-1))/(2dz),
   //   one-sided at k = 1 and nnz (derivs1.f90 / derivs2.f90 wall rows);
   // features (g * dsl, z+, dsl), normalised, through the FP64 network; the
-  // stage uses the network when the mean of -tau_ij S_ij is >= 0, and then
-  // adds the dealiased stress divergence to ru, rv, rw:
+  // stage uses the network when the mean of -tau_ij S_ij is >= 0 and, with
+  // learned_guard > 0, within a factor learned_guard of the Deardorff mean
+  // dissipation 2 nu_t S_ij S_ij (nu_t = min(0.1 dsl sqrt(e_c), xkmax) + nu,
+  // e_c = (e(k-1) + e(k)) / 2 with e(0) read as e(1)), and then adds the
+  // dealiased stress divergence to ru, rv, rw:
   //   ru += -d/dx tau11 - d/dy tau12 - (tau13w(k) - tau13w(k-1))/dz, ...
   // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on the interior w-levels and 0
   // on the walls (the wall model's stresses stay in compsgs1), plus the
@@ -772,7 +780,8 @@ struct Les {
     std::vector<std::vector<T>> g(9, std::vector<T>(ps));
     std::vector<T> wc(ps);
     const double h = (double)zl / 2.0;
-    double dsum_ = 0.0;
+    double dsum_ = 0.0, dsumd_ = 0.0;
+    const double nu_mol = (double)cfg.nu;
     std::vector<double> nuA((size_t)NZ + 2, 0.0), nuB((size_t)NZ + 2, 0.0);
     for (int iz = 1; iz <= NZ; iz++) {
       sp.xderiv(u.at(iz), g[0].data(), xk.data(), nnx, nny);
@@ -812,12 +821,19 @@ struct Les {
         const double s12 = 0.5 * ((double)g[3][q] + g[1][q]), s13 = 0.5 * ((double)g[6][q] + g[2][q]),
                      s23 = 0.5 * ((double)g[7][q] + g[5][q]);
         dsum_ += -(t[0] * s11 + t[1] * s22 + t[2] * s33 + 2.0 * (t[3] * s12 + t[4] * s13 + t[5] * s23));
+        const double ec = 0.5 * ((double)e.at(iz > 1 ? iz - 1 : 1)[q] + (double)e.at(iz)[q]);
+        const double nut = std::min(0.1 * (double)dsl * std::sqrt(std::max(ec, 0.0)), (double)xkmax) + nu_mol;
+        dsumd_ += 2.0 * nut * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23));
         nuA[iz] += t[4] * (double)g[6][q] + t[5] * (double)g[7][q];
         nuB[iz] += (double)g[6][q] * g[6][q] + (double)g[7][q] * g[7][q];
       }
     }
     learned_dissip = dsum_ / ((double)ps * NZ);
-    learned_used = learned_dissip >= 0.0 ? 1 : 0;
+    learned_dissip_d = dsumd_ / ((double)ps * NZ);
+    learned_used = learned_dissip >= 0.0 ? 1 : 0;  // NaN -> fallback
+    if (learned_guard > 0.0 && !(learned_dissip_d > 0.0 && learned_dissip <= learned_guard * learned_dissip_d &&
+                                 learned_guard * learned_dissip >= learned_dissip_d))
+      learned_used = 0;
     if (!learned_used) return;
     // stress divergence
     std::vector<T> t13w_m(ps), t13w_p(ps), t23w_m(ps), t23w_p(ps), f1(ps), f2(ps);
@@ -1290,6 +1306,18 @@ int orc_get_learned(void* hp, double* lru, double* lrv, double* lrw) {
 void orc_learned_status(void* hp, int* used, double* dissipation) {
   OrcHandle* h = (OrcHandle*)hp;
   DISPATCH(h, { if (used) *used = L.learned_used; if (dissipation) *dissipation = L.learned_dissip; });
+}
+// Deardorff mean dissipation of the last learned stage.
+double orc_learned_deardorff(void* hp) {
+  OrcHandle* h = (OrcHandle*)hp;
+  double d = 0.0;
+  DISPATCH(h, { d = L.learned_dissip_d; });
+  return d;
+}
+// Factor of the dissipation test (<= 0: sign test only).
+void orc_set_learned_guard(void* hp, double ratio) {
+  OrcHandle* h = (OrcHandle*)hp;
+  DISPATCH(h, { L.learned_guard = ratio; });
 }
 const char* orc_error(void* hp) { return ((OrcHandle*)hp)->err.c_str(); }
 

@@ -2,14 +2,16 @@
 mixed-precision Deardorff run and the mixed-precision learned-closure run
 from the same seeded initial field (512x512x256, Re_tau 590, isurface 6,
 fixed dt from CFL 0.5 of the initial field), with the mean-velocity profile,
-<u'w'> and u_rms of the two mixed forms compared with the FP64 run every
+<u'w'> and u_rms of the mixed forms compared with the FP64 run every
 `every` steps.
 
     python paes-channelflow_b200/aposteriori_c5.py [steps=1500] [every=250] [out=aposteriori_c5.json]
 
 Writes one JSON file: per checkpoint step, for each mixed form, the largest
 |U - U_fp64| over U_b, the largest <u'w'> and u_rms differences over their
-FP64 maxima, and the learned form's fallback flag of the last stage.
+FP64 maxima, and for the learned forms (default fallback test, and the sign
+test only) the last stage's (flag, network dissipation, Deardorff
+dissipation).
 """
 import importlib.util
 import json
@@ -31,12 +33,15 @@ def load():
     return P
 
 
-def run(P, precision, imodel, steps, every, dt=None, mlp=None):
-    """Mean-profile rows (U, <u'w'>, u_rms) at every checkpoint of one form."""
+def run(P, precision, imodel, steps, every, dt=None, mlp=None, guard=None):
+    """Mean-profile rows (U, <u'w'>, u_rms) at every checkpoint of one form;
+    guard: the learned closure's fallback factor (None: the default)."""
     cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=precision, imodel=imodel)
     g = P.LesGpu(cfg)
     if mlp is not None:
         g.set_mlp(mlp, RE_TAU)
+        if guard is not None:
+            g.set_learned_guard(guard)
     g.make_ic(seed=12345, amp=0.1, re_tau=RE_TAU)
     if dt is None:
         dt = g.cfl_dt(0.5)
@@ -48,7 +53,8 @@ def run(P, precision, imodel, steps, every, dt=None, mlp=None):
             mb, _ = g.stats()
             out[it] = (mb[3].copy(), mb[9].copy(), np.sqrt(np.maximum(mb[6], 0)))
             if mlp is not None:
-                used[it] = g.learned_status()[0]
+                u_, d_ = g.learned_status()
+                used[it] = (u_, d_, g.learned_deardorff())
     g.sync()
     g.close()
     return out, used, dt
@@ -64,7 +70,8 @@ def main():
     mlp = P.Mlp(z["params"], z["norm"])
     ref, _, dt = run(P, P.PREC_FP64, P.SGS_DEARDORFF, steps, every)
     forms = {"mixed_deardorff": run(P, P.PREC_MIXED, P.SGS_DEARDORFF, steps, every, dt),
-             "learned_mixed": run(P, P.PREC_MIXED, P.SGS_LEARNED, steps, every, dt, mlp)}
+             "learned_mixed": run(P, P.PREC_MIXED, P.SGS_LEARNED, steps, every, dt, mlp),
+             "learned_mixed_sign_test_only": run(P, P.PREC_MIXED, P.SGS_LEARNED, steps, every, dt, mlp, 0.0)}
     res = {"grid": [NX, NY, NZ], "re_tau": RE_TAU, "dt": dt, "steps": steps, "every": every, "forms": {}}
     for name, (prof, used, _) in forms.items():
         rows = []

@@ -166,6 +166,10 @@ struct EngineBase {
   // learned closure: attach (or with p == nullptr detach) device parameters
   virtual void set_mlp(const MlpDev* p, double re_tau) = 0;
   virtual void learned_status(int* used, double* dissipation) = 0;
+  // factor of the fallback test against the Deardorff dissipation (<= 0:
+  // the sign test only) and the Deardorff mean dissipation of the last stage
+  virtual void set_learned_guard(double ratio) = 0;
+  virtual double learned_deardorff() = 0;
   virtual void learned_features(double re_tau, float* feat) = 0;
   virtual void learn_filter(int fxy, int fz, int with_model, double* out) = 0;
   // this state := the state of `src` regridded onto this grid (redim.f90)
@@ -211,7 +215,9 @@ struct Engine : EngineBase {
   DevBuf<T> ltau;      // [8][NZ][NY][NX] tau at the cell centres + viscosity products
   DevBuf<uint4> lfeat; // [N][16] bf16 features
   DevBuf<float> fraw;  // [N][16] raw f32 features (training data)
-  DevBuf<double> lpart, lstat, lnut;
+  DevBuf<double> lpart, lstat, lnut, lpartd;
+  double lguard = 4.0;
+  static constexpr int kDdBlocks = 296;  // partial sums of k_deardorff_dissip
   DevBuf<int> lflag;
   DevBuf<T> fscr, fcp;      // filter scratch: z-averaged fine planes, coarse planes
   DevBuf<cx<T>> fsh, fch;   // filter scratch: fine and coarse spectra
@@ -445,6 +451,9 @@ struct Engine : EngineBase {
     LES_CUDA(cudaMemsetAsync(divacc.p, 0, NZ * sizeof(double), st));
     if (a.mnout_sgs) LES_CUDA(cudaMemsetAsync(sgsacc.p, 0, (size_t)NZ * 8 * sizeof(double), st));
     const T dtab2 = (T)a.dtab2;
+    // the learned closure reads the stage's start state (u, v, w and, for
+    // its fallback test, e before k_e_prep's zeta update)
+    if (learned_on()) learned_pre(a);
     with_small(NX, [&](auto cn) {
       constexpr int N = decltype(cn)::value;
       using C = RowCfg<N>;
@@ -463,7 +472,6 @@ struct Engine : EngineBase {
       launch(k_y_inverse<T, N>, dim3(cdiv(KX, CM::TC), NZ, 4), dim3(2 * CM::THREADS), 2 * CM::buf(), st, src, dst,
              KX, NZ, (T)ky0, tw);
     });
-    if (learned_on()) learned_pre();
     if (fused) {
       fused_middle(a);
     } else {
@@ -492,7 +500,8 @@ struct Engine : EngineBase {
     lfeat.alloc(2 * ps * NZ);
     lpart.alloc((size_t)nsm * kInferCtasPerSm);
     lnut.alloc((size_t)NZ * kNuChunks * 2 + NZ + 1);  // partial sums, then the face values
-    lstat.alloc(2);
+    lstat.alloc(3);
+    lpartd.alloc(kDdBlocks);
     lflag.alloc(1);
   }
   void set_mlp(const MlpDev* p, double rt) override {
@@ -503,6 +512,19 @@ struct Engine : EngineBase {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);  // captured with the previous closure
     graphs.clear();
     graph_kernels.clear();
+  }
+  void set_learned_guard(double ratio) override {
+    lguard = ratio;
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);  // captured with the previous factor
+    graphs.clear();
+  }
+  double learned_deardorff() override {
+    double v[3] = {0.0, 0.0, 0.0};
+    if (learned_on()) {
+      LES_CUDA(cudaMemcpyAsync(v, lstat.p, sizeof(v), cudaMemcpyDeviceToHost, st));
+      LES_CUDA(cudaStreamSynchronize(st));
+    }
+    return v[2];
   }
   void learned_status(int* used, double* dissipation) override {
     double v[2] = {0.0, 0.0};
@@ -652,7 +674,7 @@ struct Engine : EngineBase {
     launch(k_filt_tau<T>, dim3(cdiv(psc * NZc, 256)), dim3(256), 0, st, (const T*)fcp.p, out, (long long)(psc * NZc));
   }
   // gradients -> features -> network -> tau and the fallback flag
-  void learned_pre() {
+  void learned_pre(const StageArgs& a) {
     const size_t N = ps * NZ;
     learned_features_into(lfeat.p, false, re_tau);
     const long long ntiles = ((long long)N + 127) / 128;
@@ -660,8 +682,10 @@ struct Engine : EngineBase {
     MlpOutTau<T> out{ltau.p, (long long)N};
     launch(k_mlp_infer<MlpOutTau<T>>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, st, mlp,
            (const uint4*)lfeat.p, (long long)N, out, lpart.p, err.p);
-    launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, 1.0 / ((double)N * dsl), lflag.p,
-           lstat.p);
+    launch(k_deardorff_dissip<T>, dim3(kDdBlocks), dim3(256), 0, st, (const uint4*)lfeat.p, (const T*)(e.p + ps), mlp,
+           (long long)N, (long long)ps, (T)(0.1 * dsl), (T)a.xkmax, (T)a.nu, (T)(1.0 / dsl), lpartd.p);
+    launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, (const double*)lpartd.p,
+           (int)kDdBlocks, 1.0 / ((double)N * dsl), lguard, lflag.p, lstat.p);
   }
   // tau^ and its divergence into the new tendencies (th reuses lgy)
   void learned_post(const StageArgs& a) {

@@ -498,6 +498,16 @@ extern "C" int les_gpu_learned_status(les_handle* h, int* used, double* dissipat
   return guarded(h, [&] { h->eng->learned_status(used, dissipation); });
 }
 
+extern "C" int les_gpu_set_learned_guard(les_handle* h, double ratio) {
+  if (!h || !(ratio == ratio)) return LES_EINVAL;
+  return guarded(h, [&] { h->eng->set_learned_guard(ratio); });
+}
+
+extern "C" int les_gpu_learned_deardorff(les_handle* h, double* dissipation) {
+  if (!h || !dissipation) return LES_EINVAL;
+  return guarded(h, [&] { *dissipation = h->eng->learned_deardorff(); });
+}
+
 extern "C" int les_gpu_learn_filter(les_handle* h, int fxy, int fz, int with_model, double* out) {
   if (!h || !out) return LES_EINVAL;
   return guarded(h, [&] {

@@ -18,8 +18,11 @@
 //      and from them the normalised bf16 features (or raw f32 features);
 //   3. k_mlp_infer<MlpOutTau>: tau_ij on the tensor cores, and the per-CTA
 //      sums of the dissipation -tau_ij S_ij;
-//   4. k_learned_flag: plane-and-level mean of the dissipation (FP64, fixed
-//      order); flag = 1 when it is >= 0, else 0 (Deardorff fallback);
+//   4. k_deardorff_dissip + k_learned_flag: plane-and-level means (FP64,
+//      fixed order) of the network's dissipation -tau_ij S_ij and of the
+//      Deardorff model's 2 nu_t S_ij S_ij on the same state; flag = 1 when
+//      the network's is >= 0 and (guard > 0) within a factor guard of
+//      Deardorff's, else 0 (Deardorff fallback);
 //   ... the padded-grid kernels (their interior momentum stresses are
 //      multiplied by 1 - flag) ...
 //   5. k_row_r2c + k_col_small: tau^ at every level;
@@ -205,17 +208,62 @@ template <class T> struct MlpOutTau {
   }
 };
 
-// Mean dissipation (per-CTA sums in CTA order) -> flag and status.
-static __global__ void k_learned_flag(const double* __restrict__ part, int nparts, double inv_n_delta,
-                                      int* __restrict__ flag, double* __restrict__ status) {
+// Deardorff partial sums for the fallback test: per cell centre 2 nu_t
+// S_ij S_ij, with S from the staged bf16 features (the gradients times
+// Delta, as the network sees them), nu_t = min(c01 sqrt(e_c), xkmax) + nu
+// and e_c = (e(k-1) + e(k)) / 2, e(0) read as e(1) (e1 = e at level 1,
+// levels ps apart).  Each term is divided by Delta^2 and multiplied by
+// Delta, the scale of the network's sums (k_learned_flag divides both by
+// N Delta).  Grid-stride, 256 threads; part[blockIdx.x] = the block's sum.
+template <class T>
+__global__ void __launch_bounds__(256) k_deardorff_dissip(const uint4* __restrict__ feat, const T* __restrict__ e1,
+                                                          const MlpDev* __restrict__ P, long long N, long long ps,
+                                                          T c01, T xkmax, T nu, T inv_delta,
+                                                          double* __restrict__ part) {
+  __shared__ double red[8];
+  double acc = 0.0;
+  for (long long p = (long long)blockIdx.x * 256 + threadIdx.x; p < N; p += (long long)gridDim.x * 256) {
+    const uint4 f0 = feat[2 * p], f1 = feat[2 * p + 1];
+    const float q[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
+                        bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
+    float g[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) g[j] = q[j] * P->in_rscale[j] + P->in_shift[j];  // d_i u_j * Delta
+    const long long k = p / ps, i = p - k * ps;  // level k + 1
+    const T ec = (T)0.5 * (e1[(k > 0 ? k - 1 : 0) * ps + i] + e1[k * ps + i]);
+    const T nut = tmin(c01 * sqrt(tmax(ec, (T)0)), xkmax) + nu;
+    const float s11 = g[0], s22 = g[4], s33 = g[8];
+    const float s12 = 0.5f * (g[3] + g[1]), s13 = 0.5f * (g[6] + g[2]), s23 = 0.5f * (g[7] + g[5]);
+    const double ss = (double)s11 * s11 + (double)s22 * s22 + (double)s33 * s33 +
+                      2.0 * ((double)s12 * s12 + (double)s13 * s13 + (double)s23 * s23);
+    acc += 2.0 * (double)nut * ss * (double)inv_delta;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; w++) s += red[w];
+    part[blockIdx.x] = s;
+  }
+}
+
+// Mean dissipations (per-CTA sums in CTA order) -> flag and status
+// [network mean, flag, Deardorff mean].  guard <= 0: the sign test only.
+static __global__ void k_learned_flag(const double* __restrict__ part, int nparts, const double* __restrict__ partd,
+                                      int npartd, double inv_n_delta, double guard, int* __restrict__ flag,
+                                      double* __restrict__ status) {
   if (threadIdx.x != 0) return;
-  double s = 0.0;
+  double s = 0.0, sd = 0.0;
   for (int i = 0; i < nparts; i++) s += part[i];
-  const double mean = s * inv_n_delta;
-  const int use = (mean >= 0.0) ? 1 : 0;  // NaN -> fallback
+  for (int i = 0; i < npartd; i++) sd += partd[i];
+  const double mean = s * inv_n_delta, meand = sd * inv_n_delta;
+  int use = (mean >= 0.0) ? 1 : 0;  // NaN -> fallback
+  if (guard > 0.0 && !(meand > 0.0 && mean <= guard * meand && guard * mean >= meand)) use = 0;
   flag[0] = use;
   status[0] = mean;
   status[1] = (double)use;
+  status[2] = meand;
 }
 
 // Per-level partial sums of tau planes 6 and 7 (MlpOutTau): grid (NZ,

@@ -99,6 +99,12 @@ module les_gpu
        integer(c_int), intent(out) :: used
        real(c_double), intent(out) :: dissipation
      end function
+     ! second fallback test: factor against the Deardorff dissipation (<= 0: off)
+     integer(c_int) function les_gpu_set_learned_guard(h, ratio) bind(C, name="les_gpu_set_learned_guard")
+       import :: c_ptr, c_int, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: ratio
+     end function
      subroutine les_mlp_destroy(m) bind(C, name="les_mlp_destroy")
        import :: c_ptr
        type(c_ptr), value :: m

@@ -132,6 +132,8 @@ def lib():
         "les_mlp_adam_step": (I, [VP, VP, VP, ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(D), VP]),
         "les_gpu_set_mlp": (I, [H, VP, D]),
         "les_gpu_learned_status": (I, [H, ctypes.POINTER(I), ctypes.POINTER(D)]),
+        "les_gpu_set_learned_guard": (I, [H, D]),
+        "les_gpu_learned_deardorff": (I, [H, ctypes.POINTER(D)]),
         "les_gpu_learn_filter": (I, [H, I, I, I, VP]),
         "les_gpu_write_field": (I, [H, ctypes.c_char_p, D, I, I]),
         "les_gpu_field_wait": (I, [H]),
@@ -290,6 +292,17 @@ class LesGpu:
         d = ctypes.c_double()
         self._check(lib().les_gpu_learned_status(self.h, ctypes.byref(used), ctypes.byref(d)))
         return used.value, d.value
+
+    def set_learned_guard(self, ratio):
+        """Factor of the fallback test against the Deardorff dissipation
+        (default 4; <= 0 keeps only the sign test)."""
+        self._check(lib().les_gpu_set_learned_guard(self.h, float(ratio)))
+
+    def learned_deardorff(self):
+        """Deardorff mean dissipation of the last learned stage (synchronising)."""
+        d = ctypes.c_double()
+        self._check(lib().les_gpu_learned_deardorff(self.h, ctypes.byref(d)))
+        return d.value
 
     def learn_filter(self, fxy, fz, with_model=True):
         """Filtered coarse fields of the current state: float64 CUDA tensor

@@ -269,10 +269,12 @@ def apriori(mlp, feats, targs, norm, delta):
     return rep
 
 
-def aposteriori(first, info, params, norm, nsteps, log=print):
+def aposteriori(first, info, params, norm, nsteps, log=print, guard=0.0):
     """Coarse runs from the first filtered snapshot with the Deardorff
     closure and with the trained network; time-averaged mean U(z) over the
-    second half against the filtered fine run's mean profile."""
+    second half against the filtered fine run's mean profile.  guard: the
+    factor of the fallback test against the Deardorff dissipation for the
+    learned run (0: the sign test only, so the network itself is judged)."""
     P = _host()
     nxc, nyc, nzc = info["coarse"]
     re_tau = info["re_tau"]
@@ -288,6 +290,7 @@ def aposteriori(first, info, params, norm, nsteps, log=print):
         if imodel == 5:
             m = P.Mlp(params, norm)
             g.set_mlp(m, re_tau)
+            g.set_learned_guard(guard)
         dt = g.cfl_dt(0.5)
         prof, used, nstat = [], 0, 0
         t0 = time.time()
@@ -342,7 +345,9 @@ def run(args, log=print):
     # what the a-posteriori runs need, for evaluating later closures without a new fine run
     ev = dict(coarse=info["coarse"], re_tau=info["re_tau"], z0=info["z0"], filtered_mean_u=info["filtered_mean_u"])
     np.savez(args.out + "_eval.npz", first=first, meta=json.dumps(ev))
-    apost = aposteriori(first, info, params, norm, args.aposteriori, log) if args.aposteriori else None
+    apost = None
+    if args.aposteriori:
+        apost = aposteriori(first, info, params, norm, args.aposteriori, log, getattr(args, "guard", 0.0))
     np.savez(args.out + ".npz", params=params, norm=norm, re_tau=np.float64(args.re_tau),
              coarse=np.array(info["coarse"]), fine=np.array(info["fine"]), factor=np.array(info["factor"]))
     report = dict(data=info, training=dict(steps=steps, seconds=secs, batch=args.batch, lr=args.lr,
@@ -363,7 +368,8 @@ def evaluate(args, log=print):
     z = np.load(args.out + ".npz")
     ev = np.load(args.out + "_eval.npz")
     info = json.loads(str(ev["meta"]))
-    apost = aposteriori(ev["first"], info, z["params"], z["norm"], args.aposteriori or 4000, log)
+    apost = aposteriori(ev["first"], info, z["params"], z["norm"], args.aposteriori or 4000, log,
+                        getattr(args, "guard", 0.0))
     rp = args.out + ".json"
     rep_ = json.load(open(rp)) if os.path.exists(rp) else {}
     rep_["aposteriori"] = apost
@@ -389,6 +395,9 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--aposteriori", type=int, default=0, help="coarse steps of the a-posteriori runs (0 = skip)")
+    ap.add_argument("--guard", type=float, default=0.0,
+                    help="fallback factor against the Deardorff dissipation in the a-posteriori learned run "
+                         "(0 = sign test only: the network itself is judged)")
     ap.add_argument("--resolved-only", action="store_true",
                     help="targets without the fine run's own model stress")
     ap.add_argument("--out", default=os.path.join(HERE, "weights", "sgs_c4"))

@@ -24,13 +24,18 @@ def params():
     return P, N
 
 
-def learned_pair(product, sign, precision=8, nx=32, ny=32, nz=16):
+def learned_pair(product, sign, precision=8, nx=32, ny=32, nz=16, guard=0.0):
+    """Oracle and GPU handle with the seeded network; guard = the factor of
+    the fallback test against the Deardorff dissipation (0: the sign test
+    only, so that the seeded network's stresses are exercised)."""
     o, g, f = make_pair(product, nx, ny, nz, precision=precision, imodel=5, re_tau=RE_TAU)
     P, N = params()
     N[22:28] *= sign
     o.set_mlp(P, N, RE_TAU)
     m = product.Mlp(P, N)
     g.set_mlp(m, RE_TAU)
+    o.set_learned_guard(guard)
+    g.set_learned_guard(guard)
     return o, g, m, f
 
 
@@ -89,6 +94,44 @@ def test_anti_dissipative_network_reproduces_deardorff(gpu_lib, product):
     a, b = g.download(), d.download()
     for k in "uvwep":
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("guard", [4.0, 10.0, 1e6])
+def test_dissipation_guard_matches_oracle(gpu_lib, product, guard):
+    """The second fallback test: the Deardorff mean dissipation and the
+    decision agree with the oracle's; a rejected network reproduces the
+    Deardorff stage bit for bit."""
+    sign = dissipative_sign(product)
+    o, g, m, f = learned_pair(product, sign, guard=guard)
+    o.stage(0, 1, 1)
+    g.stage(0, True, 1)
+    used_o, dis_o = o.learned_status()
+    used_g, dis_g = g.learned_status()
+    dd_o, dd_g = o.learned_deardorff(), g.learned_deardorff()
+    assert dd_o > 0 and abs(dd_g - dd_o) <= 0.02 * dd_o
+    ratio = max(dis_o / dd_o, dd_o / dis_o)
+    if abs(ratio / guard - 1.0) > 0.1:  # decisions near the threshold may differ by rounding
+        assert used_g == used_o == (1 if ratio <= guard else 0)
+    if used_g == 0:
+        _, d, _ = make_pair(product, 32, 32, 16, imodel=3, re_tau=RE_TAU)
+        d.stage(0, True, 1)
+        a, b = g.download(), d.download()
+        for k in "uvwep":
+            assert np.array_equal(a[k], b[k]), k
+
+
+def test_guard_is_on_by_default(gpu_lib, product):
+    o, g, f = make_pair(product, 16, 16, 8, imodel=5, re_tau=RE_TAU)
+    P, N = params()
+    m = product.Mlp(P, N)
+    g.set_mlp(m, RE_TAU)
+    o.set_mlp(P, N, RE_TAU)
+    o.stage(0, 1, 1)
+    g.stage(0, True, 1)
+    used_o, _ = o.learned_status()
+    assert g.learned_status()[0] == used_o  # both apply the default factor 4
+    with pytest.raises(product.LesError):
+        g.set_learned_guard(float("nan"))
 
 
 def test_learned_graph_step_matches_stages(gpu_lib, product):

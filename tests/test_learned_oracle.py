@@ -34,19 +34,25 @@ def np_learned(cfg, fl, P, N):
     tau = (y * N[22:28] + N[28:34]).T.reshape(6, NZ, NY, NX)
     g = LN.gradients(u, v, w, cfg.xl, cfg.yl, cfg.zl)
     dz = cfg.zl / NZ
-    nut = LN.network_viscosity(g, tau, dz * dz / cfg.dt / 5.0)
-    return LN.dissipation(g, tau), LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl, u, v, nut)
+    xkmax = dz * dz / cfg.dt / 5.0
+    nut = LN.network_viscosity(g, tau, xkmax)
+    dsl = (cfg.xl / NX * cfg.yl / NY * dz) ** (1.0 / 3.0)
+    dis_d = LN.deardorff_dissipation(g, fl["e"], dsl, xkmax)
+    return LN.dissipation(g, tau), dis_d, LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl, u, v, nut)
 
 
+@pytest.mark.parametrize("guard", [0.0, 4.0, 1e6])
 @pytest.mark.parametrize("sign", [1.0, -1.0])
-def test_learned_prepare_matches_numpy(sign):
+def test_learned_prepare_matches_numpy(sign, guard):
     cfg, o, fl, P, N = make_case(sign)
     o.set_mlp(P, N, RE_TAU)
+    o.set_learned_guard(guard)
     o.stage(0, 0, 1)
     used, dis = o.learned_status()
-    dis_np, (lru, lrv, lrw) = np_learned(cfg, fl, P, N)
+    dis_np, dis_d_np, (lru, lrv, lrw) = np_learned(cfg, fl, P, N)
     assert abs(dis - dis_np) <= 1e-9 * abs(dis_np)
-    assert used == (1 if dis_np >= 0 else 0)
+    assert abs(o.learned_deardorff() - dis_d_np) <= 1e-9 * abs(dis_d_np) and dis_d_np > 0
+    assert used == LN.network_used(dis_np, dis_d_np, guard)
     if used:
         a, b, c = o.learned_divergence()
         for x, y in ((a, lru), (b, lrv), (c, lrw)):
@@ -58,6 +64,7 @@ def test_anti_dissipative_network_falls_back_to_deardorff():
     for sign in (1.0, -1.0):
         cfg, o, fields, P, N = make_case(sign)
         o.set_mlp(P, N, RE_TAU)
+        o.set_learned_guard(0.0)
         o.stage(0, 0, 1)
         used, dis = o.learned_status()
         if used:
