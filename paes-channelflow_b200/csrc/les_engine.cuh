@@ -217,7 +217,7 @@ struct Engine : EngineBase {
   DevBuf<float> fraw;  // [N][16] raw f32 features (training data)
   DevBuf<double> lpart, lstat, lnut, lpartd;
   double lguard = 4.0;
-  static constexpr int kDdBlocks = 296;  // partial sums of k_deardorff_dissip
+  static constexpr int kDdBlocks = 4;  // blocks per level of k_deardorff_dissip (partial sums 4 * NZ)
   DevBuf<int> lflag;
   DevBuf<T> fscr, fcp;      // filter scratch: z-averaged fine planes, coarse planes
   DevBuf<cx<T>> fsh, fch;   // filter scratch: fine and coarse spectra
@@ -501,7 +501,7 @@ struct Engine : EngineBase {
     lpart.alloc((size_t)nsm * kInferCtasPerSm);
     lnut.alloc((size_t)NZ * kNuChunks * 2 + NZ + 1);  // partial sums, then the face values
     lstat.alloc(3);
-    lpartd.alloc(kDdBlocks);
+    lpartd.alloc((size_t)kDdBlocks * NZ);
     lflag.alloc(1);
   }
   void set_mlp(const MlpDev* p, double rt) override {
@@ -682,10 +682,10 @@ struct Engine : EngineBase {
     MlpOutTau<T> out{ltau.p, (long long)N};
     launch(k_mlp_infer<MlpOutTau<T>>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, st, mlp,
            (const uint4*)lfeat.p, (long long)N, out, lpart.p, err.p);
-    launch(k_deardorff_dissip<T>, dim3(kDdBlocks), dim3(256), 0, st, (const uint4*)lfeat.p, (const T*)(e.p + ps), mlp,
-           (long long)N, (long long)ps, (T)(0.1 * dsl), (T)a.xkmax, (T)a.nu, (T)(1.0 / dsl), lpartd.p);
+    launch(k_deardorff_dissip<T>, dim3(kDdBlocks, NZ), dim3(256), 0, st, (const uint4*)lfeat.p, (const T*)(e.p + ps),
+           mlp, (int)ps, (T)(0.1 * dsl), (T)a.xkmax, (T)a.nu, (T)(1.0 / dsl), lpartd.p);
     launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, (const double*)lpartd.p,
-           (int)kDdBlocks, 1.0 / ((double)N * dsl), lguard, lflag.p, lstat.p);
+           kDdBlocks * NZ, 1.0 / ((double)N * dsl), lguard, lflag.p, lstat.p);
   }
   // tau^ and its divergence into the new tendencies (th reuses lgy)
   void learned_post(const StageArgs& a) {

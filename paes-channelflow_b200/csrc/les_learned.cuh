@@ -214,23 +214,29 @@ template <class T> struct MlpOutTau {
 // and e_c = (e(k-1) + e(k)) / 2, e(0) read as e(1) (e1 = e at level 1,
 // levels ps apart).  Each term is divided by Delta^2 and multiplied by
 // Delta, the scale of the network's sums (k_learned_flag divides both by
-// N Delta).  Grid-stride, 256 threads; part[blockIdx.x] = the block's sum.
+// N Delta).  Grid (gridDim.x, NZ): blockIdx.y = level - 1, a grid-stride
+// over the level's ps points; part[level][blockIdx.x] = the block's sum.
 template <class T>
 __global__ void __launch_bounds__(256) k_deardorff_dissip(const uint4* __restrict__ feat, const T* __restrict__ e1,
-                                                          const MlpDev* __restrict__ P, long long N, long long ps,
-                                                          T c01, T xkmax, T nu, T inv_delta,
-                                                          double* __restrict__ part) {
+                                                          const MlpDev* __restrict__ P, int ps, T c01, T xkmax,
+                                                          T nu, T inv_delta, double* __restrict__ part) {
   __shared__ double red[8];
+  const int k = blockIdx.y;
+  const T* ek = e1 + (size_t)k * ps;
+  const T* em = e1 + (size_t)(k > 0 ? k - 1 : 0) * ps;  // e(0) read as e(1)
+  const uint4* fk = feat + (size_t)2 * k * ps;
+  float rs[9], sh[9];
+#pragma unroll
+  for (int j = 0; j < 9; j++) { rs[j] = P->in_rscale[j]; sh[j] = P->in_shift[j]; }
   double acc = 0.0;
-  for (long long p = (long long)blockIdx.x * 256 + threadIdx.x; p < N; p += (long long)gridDim.x * 256) {
-    const uint4 f0 = feat[2 * p], f1 = feat[2 * p + 1];
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < ps; i += gridDim.x * 256) {
+    const uint4 f0 = fk[2 * i], f1 = fk[2 * i + 1];
     const float q[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
                         bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
     float g[9];
 #pragma unroll
-    for (int j = 0; j < 9; j++) g[j] = q[j] * P->in_rscale[j] + P->in_shift[j];  // d_i u_j * Delta
-    const long long k = p / ps, i = p - k * ps;  // level k + 1
-    const T ec = (T)0.5 * (e1[(k > 0 ? k - 1 : 0) * ps + i] + e1[k * ps + i]);
+    for (int j = 0; j < 9; j++) g[j] = q[j] * rs[j] + sh[j];  // d_i u_j * Delta
+    const T ec = (T)0.5 * (em[i] + ek[i]);
     const T nut = tmin(c01 * sqrt(tmax(ec, (T)0)), xkmax) + nu;
     const float s11 = g[0], s22 = g[4], s33 = g[8];
     const float s12 = 0.5f * (g[3] + g[1]), s13 = 0.5f * (g[6] + g[2]), s23 = 0.5f * (g[7] + g[5]);
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(256) k_deardorff_dissip(const uint4* __restric
   if (threadIdx.x == 0) {
     double s = 0.0;
     for (int w = 0; w < 8; w++) s += red[w];
-    part[blockIdx.x] = s;
+    part[(size_t)k * gridDim.x + blockIdx.x] = s;
   }
 }
 
