@@ -41,7 +41,7 @@ extern "C" {
 #define LES_ESTATE    7  /* entry points called out of order */
 #define LES_ENOTBUILT 8  /* CUDA kernels unavailable (no device / not built) */
 
-/* Sub-grid closure (parameters.f90:126-131 numbering for 3 and 4). */
+/* Sub-grid closure (parameters.f90:27-35 numbering for 3 and 4). */
 #define LES_SGS_DEARDORFF 3  /* Moeng (1984) TKE model, imodel=3 */
 #define LES_SGS_SMAG      4  /* Smagorinsky, imodel=4 */
 #define LES_SGS_LEARNED   5  /* learned per-point closure with Deardorff fallback */
@@ -96,9 +96,9 @@ int les_gpu_download(les_handle* h, void* u, void* v, void* w, void* e, void* p,
 /* Regridding (replaces the offline program redim.f90 plus the restart that
  * reads its output): dst's state (u, v, w, e, p) becomes src's state moved
  * onto dst's grid -- redim's linear z interpolation from src's levels
- * (interpol, redim.f90:214-287), spectral truncation / zero padding in x
- * and y (subroutine redim, redim.f90:292-327), e clamped to [1e-10, plane
- * maximum] (redim.f90:276-277), then the restart's deal of u, v, w, e
+ * (interpol, redim.f90:202-269), spectral truncation / zero padding in x
+ * and y (subroutine redim, redim.f90:277-318), e clamped to [1e-10, plane
+ * maximum] (redim.f90:262-263), then the restart's deal of u, v, w, e
  * (les.F90:185-190) and w(nnz) = 0.  Both handles: same precision, device
  * and domain lengths (xl, yl, zl), else LES_EINVAL; any nnx, nny, nnz
  * each.  Synchronous; src is only read.  dst's tendencies are left as they
@@ -113,7 +113,7 @@ int les_gpu_download_tendencies(les_handle* h, void* ru, void* rv, void* rw,
 /* Per-stage entry points, called in this order for istage = 1..3 exactly as
  * les.F90:254-285 calls the Fortran routines.
  *   les_gpu_lower   -> lower  (lowerbc.f90:1-20)
- *   les_gpu_upper   -> upper  (upperbc.f90:178-207)
+ *   les_gpu_upper   -> upper  (upperbc.f90:1-30)
  *   les_gpu_comp1   -> comp1  (comp1.f90:1-188) with derivs1/2, compadv1,
  *                      complen, compsgs1, compsgs3, sufsim, sufsim_upper,
  *                      expand/compress (filter_fftw.f90:254-308)
@@ -160,7 +160,7 @@ int les_gpu_sync(les_handle* h, double timeout_s);
  * u, v, w drawn from SplitMix64 streams seeded with seed+0,1,2 in
  * column-major order, e = e0, then deal() and one divergence projection
  * (comprhs + press + comp2 with dtab1 = 1).  Replaces initvel
- * (init.f90:248-312), whose same-seed-per-level recipe is not reproducible
+ * (init.f90:50-114), whose same-seed-per-level recipe is not reproducible
  * across compilers. */
 int les_gpu_make_ic(les_handle* h, unsigned long long seed, double ub,
                     double amp, double utau, double e0);

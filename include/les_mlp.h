@@ -3,7 +3,7 @@
  * perceptron evaluated and trained on the sm_100a tensor cores.
  *
  * The closure has no counterpart in the reference: it replaces the eddy
- * viscosity of complen.f90:69-96 and the stresses of compsgs1.f90:104-156
+ * viscosity of complen.f90:1-28 and the stresses of compsgs1.f90:1-53
  * (tau_ij = -2 nu_t S_ij) with tau_ij predicted from the local resolved
  * velocity gradients.  The solver uses it when its configuration has
  * imodel = LES_SGS_LEARNED (les_gpu.h) and a network is attached with

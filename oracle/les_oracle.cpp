@@ -396,7 +396,7 @@ struct Les {
     planes(WX, 3); planes(WY, 3); planes(WZ, 4); planes(XKK, 3); planes(ALK, 3); planes(SHEAR, 3);
     EX.assign(pb, 0); EY.assign(pb, 0); tauuu.assign(pb, 0); tauuv.assign(pb, 0); tauvv.assign(pb, 0);
     planes(tauww, 2); planes(tauuw, 2); planes(tauvw, 2);
-    // alk is allocated but never assigned in the reference (complen.f90:89);
+    // alk is allocated but never assigned in the reference (complen.f90:21);
     // Deardorff's neutral length scale l = dsl is used (consistent with
     // ceps = 0.93/dsl, les.F90:120).
     for (auto& a : ALK) std::fill(a.begin(), a.end(), dsl);
@@ -404,7 +404,7 @@ struct Les {
     initwave();
   }
 
-  // initwave (init.f90:202-242)
+  // initwave (init.f90:4-44)
   void initwave() {
     xkb.resize(nnxb); ykb.resize(nnyb); xk.resize(nnx); yk.resize(nny);
     for (int ix = 1; ix <= nnxb; ix++) {
@@ -438,7 +438,7 @@ struct Les {
     std::fill_n(w.at(0), ps, (T)0);
     std::copy_n(e.at(1), ps, e.at(0));
   }
-  // upper (upperbc.f90:178-207)
+  // upper (upperbc.f90:1-30)
   void upper() {
     for (int iz = nnz + 1; iz <= nnz + 2; iz++) std::fill_n(u.at(iz), ps, (T)0);
     for (int iz = nnz + 1; iz <= nnz + 2; iz++) std::fill_n(v.at(iz), ps, (T)0);
@@ -447,7 +447,7 @@ struct Les {
     std::fill_n(rw.at(nnz), ps, (T)0);
   }
 
-  // derivsbot (comp1.f90:200-265) for iz = istart = 1, kb = 0.
+  // derivsbot (derivs1.f90:1-66) for iz = istart = 1, kb = 0.
   void derivsbot(int iz, int lm1, int l, int nm1, int n, int np1) {
     xd(UB(0), UX[n].data()); xd(UB(1), UX[np1].data());
     yd(UB(0), UY[n].data()); yd(UB(1), UY[np1].data());
@@ -471,7 +471,7 @@ struct Les {
     UZ[lm1] = UZ[l];
     VZ[lm1] = VZ[l];
   }
-  // derivs (comp1.f90:271-312), kb = 0.
+  // derivs (derivs2.f90:1-42), kb = 0.
   void derivs(int iz, int l, int lp1, int np2) {
     if (iz < nnz - 1) {
       xd(UB(2), UX[np2].data()); yd(UB(2), UY[np2].data());
@@ -536,7 +536,7 @@ struct Les {
     }
   }
 
-  // complen (complen.f90:69-96) for ring slot l, ebuf offset kb.
+  // complen (complen.f90:1-28) for ring slot l, ebuf offset kb.
   void complen(int l, int kb, int n, int np1) {
     T* sh = SHEAR[l].data();
     T* xk_ = XKK[l].data();
@@ -560,7 +560,7 @@ struct Les {
 
   // sufsim (lowerbc.f90:25-165) on ubuf(0), vbuf(0) = level 1.
   void sufsim(int km1) { wall(true, km1); }
-  // sufsim_upper (upperbc.f90:210-337) on level nnz.
+  // sufsim_upper (upperbc.f90:33-160) on level nnz.
   void sufsim_upper(int k) { wall(false, k); }
 
   void wall(bool lowerwall, int slot) {
@@ -680,7 +680,7 @@ struct Les {
     }
   }
 
-  // compsgs1 (compsgs1.f90:104-156), kb = 0.
+  // compsgs1 (compsgs1.f90:1-53), kb = 0.
   void compsgs1(int iz, int j, int jp1, int k, int km1, int l, int lm1, int lp1, int nm1, int n, int np1,
                 int np2) {
     const T mom = sgs_mom;
@@ -710,7 +710,7 @@ struct Les {
     }
   }
 
-  // compsgs3 (compsgs3.f90:166-245), kb = 0.
+  // compsgs3 (compsgs3.f90:1-80), kb = 0.
   void compsgs3(int iz, int j, int jp1, int k, int km1, int l, int lm1, int lp1, bool mnout, int istage) {
     std::vector<T> f1(pb), f2(pb), tmp(pb);
     int i = iz;  // istart = 1
@@ -1005,7 +1005,7 @@ struct Les {
     }
   }
 
-  // press (press.F90:45-159), single process.
+  // press (press.F90:1-115), single process.
   void press() {
     T dzdz = dz * dz;
     int hs = nnx / 2 + 1;
@@ -1069,7 +1069,7 @@ struct Les {
     }
   }
 
-  // comp2 (comp2.f90:224-268)
+  // comp2 (comp2.f90:1-45)
   void comp2() {
     std::vector<T> pl(ps), f(ps);
     for (int iz = 1; iz <= nnz; iz++) {
@@ -1167,7 +1167,7 @@ struct Les {
     }
   }
 
-  // spectra (spectra2.f90:87-156) of one small plane.
+  // spectra (spectra2.f90:1-70) of one small plane.
   void spectra(const T* f, double* zspecx, double* zspec2d) {
     int hs = nnx / 2 + 1;
     std::vector<cplx<T>> wv((size_t)hs * nny);

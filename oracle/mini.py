@@ -11,13 +11,13 @@ the oracle's own DFT, so the transforms are independent too.
 Boundary rules read off the reference (U = expand(u), E = max(expand(e), emin)):
   ghosts       u(0)=v(0)=0, w(-1)=w(0)=0, e(0)=e(1)        lowerbc.f90:9-18
                u,v(nnz+1..nnz+2)=0, w(nnz..nnz+2)=0,
-               e(nnz..nnz+1)=e(nnz-1), rw(nnz)=0            upperbc.f90:189-205
-  UX,UY,VX,VY  0 at L=0 and L=nnz+1, spectral otherwise     comp1.f90:228-233, 293-296
-  WZ           0 at L=0 and L=nnz+1, (W[L]-W[L-1])/dz       comp1.f90:220-221, 284, 299
-  UZ,VZ        (U[L+1]-U[L])/dz, L=1..nnz-1; copies at 0, nnz comp1.f90:223, 236, 285, 297
-  WX,WY        0 at L=0 and L=nnz, spectral otherwise       comp1.f90:225-235, 287, 300
-  EX,EY        at level iz use E[min(iz, nnz-2)]            comp1.f90:290-291 (not set for iz>=nnz-1)
-  XKK[L]       L=0..nnz from E[L] (imodel 3) or SHEAR[L]     compsgs1.f90:127-141
+               e(nnz..nnz+1)=e(nnz-1), rw(nnz)=0            upperbc.f90:12-28
+  UX,UY,VX,VY  0 at L=0 and L=nnz+1, spectral otherwise     derivs1.f90:29-33, derivs2.f90:23-26
+  WZ           0 at L=0 and L=nnz+1, (W[L]-W[L-1])/dz       derivs1.f90:21-22, derivs2.f90:14, 29
+  UZ,VZ        (U[L+1]-U[L])/dz, L=1..nnz-1; copies at 0, nnz derivs1.f90:24, 37, derivs2.f90:15, 27
+  WX,WY        0 at L=0 and L=nnz, spectral otherwise       derivs1.f90:26-27, 35-36, derivs2.f90:17-18, 30-31
+  EX,EY        at level iz use E[min(iz, nnz-2)]            derivs2.f90:20-21 (not set for iz>=nnz-1)
+  XKK[L]       L=0..nnz from E[L] (imodel 3) or SHEAR[L]     complen.f90:13-24, compsgs1.f90:22-38
 """
 import numpy as np
 
@@ -115,7 +115,7 @@ class MiniLes:
         nz, dz = self.nz, self.dz
         dzm, dzm2, todzm = 1.0 / dz, 1.0 / dz ** 2, 0.5 / dz
         xl, yl, emin = self.xl, self.yl, self.emin
-        # lower/upper ghosts (lowerbc.f90:9-18, upperbc.f90:189-205)
+        # lower/upper ghosts (lowerbc.f90:9-18, upperbc.f90:12-28)
         self.e_ghost_bot = self.e[0].copy()
         self.e_ghost_top = self.e[nz - 2].copy()
         self.e[nz - 1] = self.e_ghost_top
@@ -165,7 +165,7 @@ class MiniLes:
         else:
             XKK = {L: np.minimum(0.1 * self.dsl * np.sqrt(e_(L)), xkmax) + self.nu for L in range(0, nz + 1)}
 
-        # wall stresses (lowerbc.f90:25-165, upperbc.f90:210-337), isurface 1 and 6
+        # wall stresses (lowerbc.f90:25-165, upperbc.f90:33-160), isurface 1 and 6
         self.dudt = self.ru.sum() / self.ru.size
         self.dvdt = self.rv.sum() / self.rv.size
         self.utau_s = np.sqrt(self.zl / 2 * np.sqrt(self.dvdt ** 2 + (self.forcing - self.dudt) ** 2))

@@ -2,7 +2,7 @@
 // closure's multilayer perceptron in FP64.
 //
 // The closure has no counterpart in the reference (it replaces the eddy
-// viscosity of complen.f90:69-96 and the stresses of compsgs1.f90:104-156
+// viscosity of complen.f90:1-28 and the stresses of compsgs1.f90:1-53
 // with a network); this file is the checker for the product's tensor-core
 // kernels and for the solver's learned stage.
 //

@@ -3,18 +3,18 @@ numpy.  Test infrastructure only: the GPU regrid (les_gpu_regrid) is checked
 against it.
 
 What the reference does (redim.f90):
-  * interpol (redim.f90:214-287) walks the old levels with a window of three
+  * interpol (redim.f90:202-269) walks the old levels with a window of three
     (m, a, b) and linearly inter/extrapolates every new level from them:
     cell-centre fields (u, v, p) at zh = (izn - 1/2) dz_new from levels a, b
-    (redim.f90:251-257); face fields (w, e) at zf = izn dz_new from (m, a) or
-    (a, b) (redim.f90:259-265).  The window starts with a = level 1, b =
-    level 2, w(m) = 0 and e(m) = e(1) (redim.f90:223-229).
-  * subroutine redim (redim.f90:292-327) moves each x-y plane to the new grid
+    (redim.f90:237-243); face fields (w, e) at zf = izn dz_new from (m, a) or
+    (a, b) (redim.f90:245-251).  The window starts with a = level 1, b =
+    level 2, w(m) = 0 and e(m) = e(1) (redim.f90:207-217).
+  * subroutine redim (redim.f90:277-318) moves each x-y plane to the new grid
     through the scaled forward transform, zeroes the old x and y Nyquist
     modes, copies kx <= min(nx)/2 and ky in [0, min(ny)/2] plus the negative
     ky band (-(min(ny)/2 - 1) .. -1), and transforms back unscaled.
   * e is clamped to [1e-10, max over the plane of the interpolated e]
-    (redim.f90:276-277).
+    (redim.f90:262-263).
 A run that restarts from the output deals u, v, w, e (les.F90:185-190,
 filter_fftw.f90:316-329: zero the x and y Nyquist modes); `restart_state`
 applies that step too, plus the solver's w(nnz) = 0.
@@ -32,7 +32,7 @@ def z_table(nzold, nznew, zl):
     """Per new level izn = 1..nznew: (a, b, c, f0, f1, d) with
     centre value = B + (B - A) * c from old levels a, b (1-based) and
     face value = F1 + (F1 - F0) * d from old levels f0, f1 (0 = the wall:
-    w(0) = 0, e(0) = e(1)).  Follows interpol (redim.f90:214-270)."""
+    w(0) = 0, e(0) = e(1)).  Follows interpol (redim.f90:202-269)."""
     if nzold < 2:
         raise ValueError("redim needs at least two old levels")
     dzold, dznew = zl / nzold, zl / nznew
@@ -57,7 +57,7 @@ def z_table(nzold, nznew, zl):
 
 
 def regrid_plane(x, nxo, nyo, nyquist=True):
-    """subroutine redim (redim.f90:292-327) on one plane x[ny][nx]."""
+    """subroutine redim (redim.f90:277-318) on one plane x[ny][nx]."""
     nyi, nxi = x.shape
     if (nxi, nyi) == (nxo, nyo):
         return np.array(x, dtype=np.float64)

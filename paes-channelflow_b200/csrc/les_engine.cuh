@@ -1000,7 +1000,7 @@ struct Engine : EngineBase {
       scalars[4] = w.w[0].utau;
     }
   }
-  // spectra (spectra2.f90:87-156) of one level: the full half spectrum of
+  // spectra (spectra2.f90:1-70) of one level: the full half spectrum of
   // the physical plane on the device, the binning on the host.
   void spectra(int field, int iz, double* zx, double* z2) override {
     const int H = NX / 2 + 1;

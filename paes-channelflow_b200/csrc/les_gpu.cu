@@ -313,7 +313,7 @@ int les_gpu_download_tendencies(les_handle* h, void* ru, void* rv, void* rw, voi
 }
 
 // Ghost planes are rebuilt inside comp1 from exactly the values lower/upper
-// copy (lowerbc.f90:9-18, upperbc.f90:189-205), so these only validate.
+// copy (lowerbc.f90:9-18, upperbc.f90:12-28), so these only validate.
 int les_gpu_lower(les_handle* h) { return h ? LES_OK : LES_EINVAL; }
 int les_gpu_upper(les_handle* h) { return h ? LES_OK : LES_EINVAL; }
 

@@ -7,7 +7,7 @@
 //   ruo, rvo, rwo     tendencies of the previous stage (spectral)
 //   mu, mv, mru, mrv  FP64 shadows of the kx=ky=0 modes (mean profiles)
 //   e, re             SGS TKE and its tendency in physical space (the e
-//                     update clips at emin, comp2.f90:261)
+//                     update clips at emin, comp2.f90:38)
 // Work arrays on the 3/2-padded grid (nxb = 3nx/2, nyb = 3ny/2):
 //   "mixed" arrays    x-spectral, y-physical  [z][y][kx]  (kx < nx/2)
 //   "padded" arrays   physical                [z][y][x]
@@ -58,7 +58,7 @@ struct StageArgs {
   double zl, ugal, vgal;
 };
 
-// Wall-model scalars for one wall (lowerbc.f90:56-124 / upperbc.f90:240-299).
+// Wall-model scalars for one wall (lowerbc.f90:56-124 / upperbc.f90:63-122).
 struct WallSide {
   double u1xy, v1xy, vsfc, utau, windm, ufluc2mroot, vfluc2mroot, suflucm, svflucm;
   double moengu2mroot, moengv2mroot, auuwm, auvwm, denom;
@@ -248,7 +248,7 @@ k_col_trunc(const cx<T>* __restrict__ in, cx<T>* __restrict__ out, int KX, T sca
 // ---------------------------------------------------------------------------
 // Stage kernels
 // ---------------------------------------------------------------------------
-// lower/upper ghosts of e (lowerbc.f90:13-17, upperbc.f90:197-201), the
+// lower/upper ghosts of e (lowerbc.f90:13-17, upperbc.f90:20-24), the
 // zeta part of the stage for e (comp1.f90:131), and the x-transform of e
 // (first half of expand, filter_fftw.f90:262-263).  e has levels 0..NZ+1.
 template <class T, int NX>
@@ -380,7 +380,7 @@ k_x_inverse(Ptr8 src, Ptr12 dst, int MY, int NZ, T kx0, const cx<T>* __restrict_
 
 // yderiv of delta = max(emin - E, 0) on padded planes (column pairs),
 // added to EY.  This and k_clip_x make EX, EY the derivatives of the
-// clipped ebuf = max(expand(e), emin) (comp1.f90:109,121; derivs2.f90:19-20).
+// clipped ebuf = max(expand(e), emin) (comp1.f90:109,121; derivs2.f90:20-21).
 template <class T, int NSY>
 __global__ void __launch_bounds__(ColCfg<3 * NSY / 2, T>::THREADS)
 k_clip_y(const T* __restrict__ E, T* __restrict__ EY, int MX, T emin, T ky0, const cx<T>* __restrict__ tw) {
@@ -494,7 +494,7 @@ __global__ void k_wall_sums(const T* __restrict__ U, const T* __restrict__ V, in
   block_sum_store<8>(s, part + ((size_t)side * gridDim.x + blockIdx.x) * 8);
 }
 
-// Wall-model scalars for both walls (lowerbc.f90:56-124, upperbc.f90:240-299)
+// Wall-model scalars for both walls (lowerbc.f90:56-124, upperbc.f90:63-122)
 // and the global dudt, dvdt (lowerbc.f90:70-72) from the FP64 mean shadows.
 static __global__ void k_wall_final(const double* __restrict__ part, int nblk, const double* __restrict__ mru,
                              const double* __restrict__ mrv, StageArgs a, double P, double vk, double zody,
@@ -550,7 +550,7 @@ static __global__ void k_wall_final(const double* __restrict__ part, int nblk, c
   }
 }
 
-// Wall stress tau13, tau23 at one point (lowerbc.f90:126-161, upperbc.f90:301-335).
+// Wall stress tau13, tau23 at one point (lowerbc.f90:126-161, upperbc.f90:124-158).
 template <class T>
 __device__ __forceinline__ void wall_stress(const WallSide& w, const WallParams& wp, const StageArgs& a, int side,
                                             T U, T V, T& tu, T& tv) {
@@ -597,7 +597,7 @@ __device__ __forceinline__ void wall_stress(const WallSide& w, const WallParams&
 //   w: D=0.5(U0+U1)W0+tuw (-d/dx), G=0.5(V0+V1)W0+tvw (-d/dy), Pw
 //   e: F=0.5E0(U0+U1)-2xkk EX (-d/dx), H=0.5E0(V0+V1)-2xkk EY (-d/dy), Pe
 // in: U,UX,UY,V,VX,VY,W,WX,WY,E,EX,EY   out: A,B,C,D,G,F,H,Pu,Pv,Pw,Pe
-// stats: divz[z] (comp1.f90:145) and the SGS means (compsgs3.f90:236-243).
+// stats: divz[z] (comp1.f90:145) and the SGS means (compsgs3.f90:71-78).
 struct Ptr11 { void* p[11]; };
 template <class T>
 __global__ void __launch_bounds__(256)
@@ -808,7 +808,7 @@ k_y_forward(Ptr8 X, Ptr8 rnew, int KX, int NZ, T ky0, T scale, const cx<T>* __re
   }
 }
 
-// comp2's e update (comp2.f90:261) with re from its x-spectral rows:
+// comp2's e update (comp2.f90:38) with re from its x-spectral rows:
 // re = c2r(rem), e = max(e + dtab1*re, emin), levels 1..nnz-1.
 template <class T, int NX>
 __global__ void __launch_bounds__(RowCfg<NX>::THREADS)
@@ -854,7 +854,7 @@ k_e_update(const cx<T>* __restrict__ rem, T* __restrict__ re, T* __restrict__ e,
 }
 
 // comprhs + press + tridv for every (kx, ky) column in z, in FP64
-// (comprhs.f90:17-35, press.F90:81-145, tridv.f90:195-219).
+// (comprhs.f90:17-35, press.F90:37-101, tridv.f90:29-53).
 //   rhs = ikx (Ru + u*/dtab1) + iky (Rv + v*/dtab1) + (Q(z) - Q(z-1))/dz,
 //   Q = w*/dtab1 + Rw, u* = u - dtab2*Ru_old (comp1.f90:127).
 // Thomas sweeps use scratch d[z][mode], r[z][mode].
@@ -913,7 +913,7 @@ __global__ void k_press(const cx<T>* __restrict__ uh, const cx<T>* __restrict__ 
   }
 }
 
-// comp2 (comp2.f90:238-266) in spectral space, FP64 arithmetic:
+// comp2 (comp2.f90:15-43) in spectral space, FP64 arithmetic:
 //   Ru' = Ru - ikx p, Rv' = Rv - iky p, Rw' = Rw - (p(z+1)-p(z))/dz (mean 0),
 //   u = u* + dtab1 Ru', ..., w plane mean removed.  The kx=ky=0 modes of u, v
 //   and their tendencies live in the FP64 shadows mu, mv, mru, mrv.
@@ -1177,7 +1177,7 @@ k_op_yderiv(const T* __restrict__ in, T* __restrict__ out, int n1, T k0, const c
   });
 }
 
-// tridv (tridv.f90:167-221) for one right-hand side per thread; bdar is
+// tridv (tridv.f90:1-55) for one right-hand side per thread; bdar is
 // (ny, n, 4) column-major.
 static __global__ void k_op_tridv(double* bdar, int ny, int n) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,6 +1,6 @@
 // les_regrid.cuh -- spectral regridding of the state onto another grid, the
-// device form of the reference's redim.f90 (interpol redim.f90:214-287 and
-// subroutine redim redim.f90:292-327) followed by the dealiasing a restarted
+// device form of the reference's redim.f90 (interpol redim.f90:202-269 and
+// subroutine redim redim.f90:277-318) followed by the dealiasing a restarted
 // run applies (les.F90:185-190).
 //
 // The state is spectral in x-y (u^ = FFT2(u) / (nx ny), kx < nx/2), so the
@@ -12,7 +12,7 @@
 // which replays redim's walk over the old levels.  e is physical: its planes
 // are interpolated in z, transformed on the old grid, copied, transformed
 // back on the new grid, clamped to [1e-10, plane max of the interpolated e]
-// (redim.f90:276-277) and dealt.
+// (redim.f90:262-263) and dealt.
 #pragma once
 #include "les_kernels.cuh"
 
@@ -26,7 +26,7 @@ struct RegridLevel {
   double c, d;
 };
 
-// Host replay of interpol's walk (redim.f90:214-270) for nznew new levels.
+// Host replay of interpol's walk (redim.f90:202-269) for nznew new levels.
 inline std::vector<RegridLevel> regrid_table(int nzold, int nznew, double zl) {
   std::vector<RegridLevel> t(nznew);
   const double dzold = zl / nzold, dznew = zl / nznew;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256) k_plane_max(const T* __restrict__ a, size
   if (threadIdx.x == 0) out[blockIdx.x] = red[0];
 }
 
-// e = min(emax(level), max(e, 1e-10)) on cnt planes (redim.f90:276-277).
+// e = min(emax(level), max(e, 1e-10)) on cnt planes (redim.f90:262-263).
 // Grid (cdiv(P, 256), cnt).
 template <class T>
 __global__ void k_regrid_eclamp(T* __restrict__ e, const double* __restrict__ emax, size_t P) {

@@ -469,7 +469,7 @@ def deal(a):
 
 
 def tridv(bdar):
-    """tridv (tridv.f90:167-221) on a float64 CUDA tensor shaped (4, n, ny)."""
+    """tridv (tridv.f90:1-55) on a float64 CUDA tensor shaped (4, n, ny)."""
     out = bdar.clone()
     _, n, ny = out.shape
     _op_check(lib().les_op_tridv(out.data_ptr(), ny, n, 8, _stream(out)))
