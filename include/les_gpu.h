@@ -227,7 +227,12 @@ int les_op_tridv(void* bdar, int ny, int n, int real_bytes, void* stream);
  * each for real_bytes = 8, 8 for 4) must fit in 16 MiB, else LES_EINVAL.
  * Every device that loads the library keeps the array until exit; calls
  * share it, so calls that overlap on the GPU race; the first call on each
- * device does a one-time set-up and must come before any stream capture. */
+ * device does a one-time set-up and must come before any stream capture.
+ * Under CUDA's lazy module loading (the default since CUDA 12.2) the array
+ * is placed in device memory by that first call, not when the library is
+ * loaded: a host that reserves all free device memory up front must make
+ * its first call on each device before reserving, or run with
+ * CUDA_MODULE_LOADING=EAGER. */
 int les_op_expand_noalloc(const void* xsmall, void* xlarge, int nx, int ny,
                           int howmany, int real_bytes, void* stream);
 
@@ -238,7 +243,11 @@ int les_op_expand_noalloc(const void* xsmall, void* xlarge, int nx, int ny,
  *   divgls, fcor, ugtop, ugbot, vgtop, vgbot | then per level iz = 1..nnz:
  *   u, v, w, e, p(1:nnx,1:nny) of level iz.
  * real_bytes: 4 for the shipped build, 8 for -fdefault-real-8 (integers are
- * 4 bytes in both).  divgls..vgbot are written as 0 (not used by this path).
+ * 4 bytes in both).  Record 3 is not used by this path; it is written as
+ * divgls = 0, fcor = 1e-4 (default.f90:23), ugtop = ugbot = 2 ugal and
+ * vgtop = vgbot = 2 vgal, so that the post-processing programs' formula
+ * ugal = (max(0, max(ugtop, ugbot)) + min(0, min(ugtop, ugbot))) / 2
+ * (calc_pdf.f90:99-100) gives back the run's Galilean shift.
  *
  * les_gpu_write_field: downloads the state (synchronous on the device) and
  * writes the file; with async != 0 the file is written by a host thread and

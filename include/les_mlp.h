@@ -54,6 +54,18 @@ const char* les_mlp_last_error(const les_mlp* m);
 int les_mlp_set_params(les_mlp* m, const float* params, const float* norm);
 int les_mlp_get_params(les_mlp* m, float* params, float* norm);
 
+/* Limit of each wait for a tensor-core MMA in this network's kernels
+ * (inference in les_mlp_forward and in the solver's learned stage,
+ * training in les_mlp_loss_grad / les_mlp_adam_step); default 1 s, range
+ * [0, 60] s.  A wait that runs out makes the kernel give up its tiles,
+ * drain the outstanding MMA (bounded by a fixed 1 s), release its tensor
+ * memory and return; the host then sees LES_ETIMEOUT (les_mlp_loss_grad,
+ * les_mlp_adam_step, or les_gpu_sync of a handle using the network) and the
+ * CUDA context stays usable.  0 gives up at the first poll that finds an
+ * MMA unfinished, which tests use to exercise that path.  Synchronises the
+ * device. */
+int les_mlp_set_wait_limit(les_mlp* m, double seconds);
+
 /* y[n][8] = network(feat[n][16]) in normalised units (asynchronous). */
 int les_mlp_forward(les_mlp* m, const void* feat, long long n, float* y, void* stream);
 

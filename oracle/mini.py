@@ -165,24 +165,45 @@ class MiniLes:
         else:
             XKK = {L: np.minimum(0.1 * self.dsl * np.sqrt(e_(L)), xkmax) + self.nu for L in range(0, nz + 1)}
 
-        # wall stresses (lowerbc.f90:25-165, upperbc.f90:33-160), isurface 1 and 6
+        # wall stresses (lowerbc.f90:25-165, upperbc.f90:33-160), isurface 1..6
         self.dudt = self.ru.sum() / self.ru.size
         self.dvdt = self.rv.sum() / self.rv.size
         self.utau_s = np.sqrt(self.zl / 2 * np.sqrt(self.dvdt ** 2 + (self.forcing - self.dudt) ** 2))
 
         def wall(L, sg):
-            u1, v1 = U[L].mean(), V[L].mean()
+            """sg = -1 lower wall (sufsim), +1 upper wall (sufsim_upper)."""
+            U0, V0 = U[L], V[L]
+            u1, v1 = U0.mean(), V0.mean()
+            wind = np.sqrt(U0 * U0 + V0 * V0)
+            windm = max(wind.mean(), 0.0, 0.01)   # max(windm, ufree), max(windm, 0.01); ufree = 0
             vsfc = max(np.sqrt(u1 * u1 + v1 * v1), 0.01)
             ut = vsfc * 0.4 / self.zody
+            ut2 = ut * ut
+            uf, vf = U0 - u1, V0 - v1             # ufluc, vfluc (ugal = 0)
+            th = np.arccos(min(max(u1 / vsfc, -1.0), 1.0))
+            au = sg * ut2 * np.cos(th)             # auuwm, auvwm (lowerbc.f90:88-89, upperbc.f90:87-88)
+            av = sg * ut2 * np.sin(th) * np.copysign(1.0, v1)
             if self.isurface == 1:
-                return sg * ut * ut / vsfc * U[L], sg * ut * ut / vsfc * V[L], ut
-            if self.isurface == 6:
-                au = -self.zl / 2 * (self.forcing - self.dudt)
-                av = -self.zl / 2 * (-self.dvdt)
-                if sg < 0:
-                    return au - ut * self.utau_s * (U[L] - u1) / vsfc, av - ut * self.utau_s * (V[L] - v1) / vsfc, ut
-                return -au + ut * self.utau_s * (U[L] - u1) / vsfc, -av + ut * self.utau_s * (V[L] - v1) / vsfc, ut
-            raise NotImplementedError("mini oracle: isurface 1 and 6 only")
+                return sg * ut2 / vsfc * U0, sg * ut2 / vsfc * V0, ut
+            if self.isurface == 2:
+                c = sg * ut2 / (windm * vsfc)
+                return c * (windm * uf + wind * u1), c * (windm * vf + wind * v1), ut
+            if self.isurface == 3:
+                return (au - sg * 0.35 * uf * ut2 / np.sqrt((uf * uf).mean()),
+                        av - sg * 0.35 * vf * ut2 / np.sqrt((vf * vf).mean()), ut)
+            sf = wind - windm
+            if self.isurface == 4:
+                den = np.sqrt((windm * u1 + (uf * sf).mean()) ** 2 + (windm * v1 + (vf * sf).mean()) ** 2)
+                return sg * ut2 * wind * U0 / den, sg * ut2 * wind * V0 / den, ut
+            if self.isurface == 5:
+                mu, mv = sf * u1 + windm * uf, sf * v1 + windm * vf
+                root = np.sqrt((mu * mu).mean())  # moengv2m is built from moengu2 (lowerbc.f90:121)
+                return au - sg * 0.35 * ut2 * mu / root, av - sg * 0.35 * ut2 * mv / root, ut
+            a6u = -self.zl / 2 * (self.forcing - self.dudt)
+            a6v = -self.zl / 2 * (-self.dvdt)
+            if sg < 0:
+                return a6u - ut * self.utau_s * uf / vsfc, a6v - ut * self.utau_s * vf / vsfc, ut
+            return -a6u + ut * self.utau_s * uf / vsfc, -a6v + ut * self.utau_s * vf / vsfc, ut
 
         TUW, TVW = {}, {}
         TUW[0], TVW[0], self.utau_lower = wall(1, -1.0)

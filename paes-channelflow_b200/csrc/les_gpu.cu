@@ -367,9 +367,11 @@ int les_gpu_sync(les_handle* h, double timeout_s) {
   int flags = 0;
   rc = guarded(h, [&] { flags = h->eng->read_error(); });
   if (rc) return rc;
+  // a tensor-core wait that ran out leaves the network's stresses unset, so
+  // it is reported before the NaN or wall-model states it may cause
+  if (flags & ERR_MMA_TIMEOUT) { h->err = "a tensor-core MMA did not complete within its wait limit"; return LES_ETIMEOUT; }
   if (flags & ERR_UTAU) { h->err = "stop because utau > 10 (wall model blow-up guard)"; return LES_EUTAU; }
   if (flags & ERR_NAN) { h->err = "NaN/Inf in the state"; return LES_ENAN; }
-  if (flags & ERR_MMA_TIMEOUT) { h->err = "a tensor-core MMA did not complete within its wait limit"; return LES_ETIMEOUT; }
   return LES_OK;
 }
 
@@ -641,7 +643,16 @@ extern "C" int les_gpu_write_field(les_handle* h, const char* path, double time,
       std::memcpy(r1.data() + o, d, 12);
       put_real(r1, c.xl, rb); put_real(r1, c.yl, rb); put_real(r1, c.zl, rb);
       put_real(r2, c.dt, rb); put_real(r2, c.z0, rb); put_real(r2, utau, rb);
-      for (int i = 0; i < 6; i++) put_real(r3, 0.0, rb);  // divgls, fcor, ugtop, ugbot, vgtop, vgbot
+      // divgls, fcor, ugtop, ugbot, vgtop, vgbot.  The post-processing
+      // programs take the run's Galilean shift from this record as
+      // ugal = (max(0, max(ugtop, ugbot)) + min(0, min(ugtop, ugbot))) / 2
+      // (calc_pdf.f90:99-100, calc_spectra.f90:130-131,
+      // calc_integral_ls.f90:87-88); ugtop = ugbot = 2 ugal gives back ugal
+      // for either sign (likewise v).  fcor is default.f90:23's value.
+      put_real(r3, 0.0, rb);
+      put_real(r3, 1e-4, rb);
+      put_real(r3, 2.0 * c.ugal, rb); put_real(r3, 2.0 * c.ugal, rb);
+      put_real(r3, 2.0 * c.vgal, rb); put_real(r3, 2.0 * c.vgal, rb);
       ok = write_record(f, {{r1.data(), r1.size()}}) && write_record(f, {{r2.data(), r2.size()}}) &&
            write_record(f, {{r3.data(), r3.size()}});
       const size_t pl = ps * rb;

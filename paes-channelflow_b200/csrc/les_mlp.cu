@@ -23,6 +23,7 @@ struct les_mlp {
   DevBuf<int> err;
   std::vector<float> norm = std::vector<float>(kMlpNNorm, 0.f);
   int adam_step = 0;
+  unsigned long long wait_ns = kMmaWaitNs;  // MlpDev::wait_ns
   int nsm = 148;
   std::string msg;
 };
@@ -144,6 +145,7 @@ int les_mlp_create(int device, les_mlp** out) {
     LES_CUDA(cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, device));
     LES_CUDA(cudaMalloc((void**)&m->dev, sizeof(MlpDev)));
     LES_CUDA(cudaMemset(m->dev, 0, sizeof(MlpDev)));
+    LES_CUDA(cudaMemcpy(&m->dev->wait_ns, &m->wait_ns, sizeof(m->wait_ns), cudaMemcpyHostToDevice));
     for (auto* b : {&m->master, &m->m1, &m->m2, &m->grad}) b->alloc(kMlpNParam);
     m->part.alloc((size_t)m->nsm * kMlpNParam);
     m->lpart.alloc(m->nsm);
@@ -184,12 +186,22 @@ int les_mlp_set_params(les_mlp* m, const float* params, const float* norm) {
       if (!std::isfinite(norm[i])) throw std::invalid_argument("non-finite normalisation");
     MlpDev h;
     pack_params(params, norm, h);
+    h.wait_ns = m->wait_ns;
     LES_CUDA(cudaMemcpy(m->dev, &h, sizeof(MlpDev), cudaMemcpyHostToDevice));
     LES_CUDA(cudaMemcpy(m->master.p, params, kMlpNParam * sizeof(float), cudaMemcpyHostToDevice));
     LES_CUDA(cudaMemset(m->m1.p, 0, kMlpNParam * sizeof(float)));
     LES_CUDA(cudaMemset(m->m2.p, 0, kMlpNParam * sizeof(float)));
     m->norm.assign(norm, norm + kMlpNNorm);
     m->adam_step = 0;
+  });
+}
+
+int les_mlp_set_wait_limit(les_mlp* m, double seconds) {
+  if (!m || !(seconds >= 0.0 && seconds <= 60.0)) return LES_EINVAL;
+  return mlp_guard(m, [&] {
+    m->wait_ns = (unsigned long long)(seconds * 1e9);
+    LES_CUDA(cudaDeviceSynchronize());  // no kernel reads the old value any more
+    LES_CUDA(cudaMemcpy(&m->dev->wait_ns, &m->wait_ns, sizeof(m->wait_ns), cudaMemcpyHostToDevice));
   });
 }
 

@@ -31,6 +31,9 @@ constexpr int kMlpNNorm = 34;
 // offsets in the flat parameter vector: W1[64][11], b1, W2[64][64], b2, W3, b3, W4[6][64], b4
 constexpr int kPW1 = 0, kPB1 = 704, kPW2 = 768, kPB2 = 4864, kPW3 = 4928, kPB3 = 9024, kPW4 = 9088, kPB4 = 9472;
 constexpr int ERR_MMA_TIMEOUT = 4;
+// Default limit of a wait for a tensor-core MMA (MlpDev::wait_ns, settable
+// per network from the host), and the fixed limit of the wait that drains an
+// outstanding MMA after a failure, before its tensor memory is released.
 constexpr uint64_t kMmaWaitNs = 1000000000ull;  // 1 s
 
 // Device-side parameters: bf16 weight tiles in the core-matrix layout
@@ -44,6 +47,8 @@ struct MlpDev {
   float b1[64], b2[64], b3[64], b4[16];
   float in_shift[16], in_scale[16], out_scale[8], out_shift[8];
   float in_rscale[16];  // 1 / in_scale (0 where in_scale is 0)
+  unsigned long long wait_ns;  // limit of each wait for an MMA (kMmaWaitNs by default)
+  unsigned long long pad_;
 };
 static_assert(sizeof(MlpDev) % 16 == 0, "MlpDev is copied in 16-byte words");
 
@@ -154,7 +159,7 @@ __device__ __forceinline__ MlpGroup mlp_group(MlpDev* P, unsigned char* act, uin
 __device__ __forceinline__ bool mlp_tile(MlpGroup& G, const MlpDev* P, int r, uint4 f0, uint4 f1,
                                          float (&y)[16]) {
   auto wait_mma = [&]() -> bool {
-    const bool ok = tc::mbar_wait(G.mbar, G.parity, kMmaWaitNs);
+    const bool ok = tc::mbar_wait(G.mbar, G.parity, P->wait_ns);
     G.parity ^= 1;
     tc::fence_after_sync();
     return ok;
@@ -356,7 +361,7 @@ k_mlp_train(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, cons
   float db4[kMlpOut] = {0, 0, 0, 0, 0, 0};
   double lsum = 0.0;
   auto wait_mma = [&]() -> bool {
-    const bool ok = tc::mbar_wait(barp, parity, kMmaWaitNs);
+    const bool ok = tc::mbar_wait(barp, parity, P->wait_ns);
     parity ^= 1;
     tc::fence_after_sync();
     return ok;

@@ -6,8 +6,8 @@
 // driver that calls from inside a region where allocation is forbidden or
 // would serialise other streams, or an embedding whose allocator policy
 // bans hidden allocations.  les_op_expand obtains two scratch buffers with
-// cudaMallocAsync; this variant uses a static array that exists from the
-// moment the library is loaded on a device until the process exits.
+// cudaMallocAsync; this variant uses a static array that, once placed on a
+// device, stays there until the process exits.
 //
 // Limits and caveats:
 //  - capacity: kNoAllocBytes (16 MiB) per device; the scratch a call needs
@@ -21,6 +21,13 @@
 //  - the first call on each device does a one-time set-up (it looks up the
 //    array's device address and copies the twiddle tables); make that first
 //    call before any stream capture on that device.
+//  - when the array is placed: under CUDA's lazy module loading (the default
+//    since CUDA 12.2) this file's device code, the 16 MiB array and the
+//    twiddle tables are loaded onto a device by that first call's
+//    cudaGetSymbolAddress, not when the library is loaded.  That load takes
+//    device memory, so a host that reserves all free device memory up front
+//    must make its first call on each device before reserving (or run with
+//    CUDA_MODULE_LOADING=EAGER, which loads them with the CUDA context).
 //  - nothing in the array needs clearing: every scratch element a call
 //    reads is written earlier by the same call.
 #include <mutex>

@@ -119,13 +119,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Wait for phase `parity` of the barrier to complete; gives up after
-// limit_ns nanoseconds and returns false.
+// Wait for phase `parity` of the barrier to complete; gives up once limit_ns
+// nanoseconds have passed since the first unsuccessful poll and returns
+// false (limit 0: at the second unsuccessful poll).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   while (!mbar_try(bar, parity)) {
-    if (globaltimer_ns() - t0 > limit_ns) return false;
+    if (globaltimer_ns() - t0 >= limit_ns) return false;
   }
   return true;
 }

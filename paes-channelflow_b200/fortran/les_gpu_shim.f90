@@ -1,12 +1,20 @@
 ! les_gpu_shim.f90 -- Fortran binding of libles_gpu.so (include/les_gpu.h, include/les_mlp.h).
 !
-! Replaces comp1.o comp2.o compadv1.o compsgs1.o compsgs3.o derivs1.o
-! derivs2.o press.o tridv.o filter_fftw.o lowerbc.o upperbc.o complen.o in
-! LESOBJS (Makefile:11-14) so that les.F90 keeps driving the stage loop
-! (les.F90:254-285) with the same subroutine names and arguments, while the
-! domain lives on one GPU.  The storage module stays the host copy used for
-! restart files and statistics output.  Not compiled in this repository (no
-! Fortran compiler in the build image); see INTEGRATION.md.
+! Replaces comp1.o comp2.o compadv1.o compsgs1.o compsgs3.o complen.o
+! derivs1.o derivs2.o comprhs.o press.o tridv.o lowerbc.o upperbc.o and
+! compmn.o in LESOBJS (Makefile:11-14) so that les.F90 keeps driving the
+! stage loop (les.F90:254-285) with the same subroutine names and arguments
+! while the domain lives on one GPU.  filter_fftw.o and FFTW 2.x stay in the
+! link: the host still uses fft_init, deal, xderiv/yderiv (initvel,
+! init.f90:95-96) and fft_finalize once, outside the stage loop
+! (les.F90:149, 173, 185-190, 356).  The storage module stays the host copy
+! of the state for restart files; three calls are added to les.F90:
+!   les_gpu_attach  after the deal loop (les.F90:190): init + upload
+!   les_gpu_fetch   before the restart write (les.F90:331): download
+!   les_gpu_detach  before fft_finalize (les.F90:356)
+! compmn (les.F90:288) is provided here and fills meanbuf, utau, utau_s,
+! dudt and dvdt from the device.  Serial build only (no -DMPI: the GPU holds
+! the whole domain).
 module les_gpu
   use iso_c_binding
   implicit none
@@ -76,6 +84,11 @@ module les_gpu
        import :: c_ptr, c_int
        type(c_ptr), value :: h, meanbuf, scalars
      end function
+     integer(c_int) function les_gpu_sync(h, timeout_s) bind(C, name="les_gpu_sync")
+       import :: c_ptr, c_int, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: timeout_s
+     end function
      ! learned closure (include/les_mlp.h): create a network, load the
      ! parameters of a weights file (params(9478), norm(34) as real(c_float)),
      ! attach it to a handle configured with imodel = 5
@@ -115,7 +128,49 @@ module les_gpu
      end function
   end interface
 
+  ! bytes of the host's default real (4 as shipped, 8 with -fdefault-real-8)
+  integer, save :: rbytes = 8
+
 contains
+
+  ! les.F90:190, after the restart read or initvel and the deal loop:
+  ! les_gpu_init replaces setcombuf, allocate_arrays' device part, initwave
+  ! and fft_init for the stage loop; the state is uploaded once.
+  subroutine les_gpu_attach()
+    use storage
+    use parameters
+    type(les_config), target :: gcfg
+    gcfg%nnx = nnx; gcfg%nny = nny; gcfg%nnz = nnz
+    gcfg%imodel = imodel; gcfg%isurface = isurface
+    gcfg%tke_production = 0; gcfg%precision = 8; gcfg%device = 0
+    gcfg%xl = xl; gcfg%yl = yl; gcfg%zl = zl; gcfg%z0 = z0; gcfg%dt = dt
+    gcfg%cb = cb; gcfg%skc = skc; gcfg%nu = 0d0
+    gcfg%ugal = ugal; gcfg%vgal = vgal; gcfg%ufree = 0d0
+    gcfg%emin = emin; gcfg%forcing = 0.016d0
+    rbytes = storage_size(u) / 8
+    call les_check(les_gpu_init(gcfg, les_h))
+    call les_check(les_gpu_upload(les_h, c_loc(u(1,1,1)), c_loc(v(1,1,1)), c_loc(w(1,1,1)), &
+         c_loc(e(1,1,1)), c_null_ptr, int(rbytes, c_int)))
+  end subroutine les_gpu_attach
+
+  ! les.F90:331, before write_params / sav_field: the device state into the
+  ! storage module (levels 1..nnz; p into p(1:nnx,:,:))
+  subroutine les_gpu_fetch()
+    use storage
+    real, allocatable, target :: pr(:,:,:)
+    allocate(pr(nnx, nny, nnz))
+    call les_check(les_gpu_download(les_h, c_loc(u(1,1,1)), c_loc(v(1,1,1)), c_loc(w(1,1,1)), &
+         c_loc(e(1,1,1)), c_loc(pr(1,1,1)), int(rbytes, c_int)))
+    p(1:nnx, 1:nny, 1:nnz) = pr
+    deallocate(pr)
+  end subroutine les_gpu_fetch
+
+  ! les.F90:356, before fft_finalize / deallocate_arrays
+  subroutine les_gpu_detach()
+    call les_check(les_gpu_sync(les_h, -1d0))
+    call les_gpu_finalize(les_h)
+    les_h = c_null_ptr
+  end subroutine les_gpu_detach
 
   subroutine les_check(rc)
     integer(c_int), intent(in) :: rc
@@ -157,5 +212,20 @@ contains
     integer :: istart, iend
     call les_check(les_gpu_comp2(les_h, real(dtab1, c_double)))
   end subroutine comp2
+
+  ! compmn (compmn.F90:1-64) from the device: meanbuf(19, nnz) in the
+  ! allocate.f90:89-111 row order, and the wall-model scalars that
+  ! output_profiles prints (les.F90:389-407)
+  subroutine compmn(istart, iend)
+    use storage
+    integer :: istart, iend
+    real(c_double), allocatable, target :: mb(:,:)
+    real(c_double), target :: sc(5)
+    allocate(mb(19, nnz))
+    call les_check(les_gpu_stats(les_h, c_loc(mb(1,1)), c_loc(sc(1))))
+    meanbuf(1:19, istart:iend) = mb(1:19, istart:iend)
+    utau = sc(1); utau_s = sc(2); dudt = sc(3); dvdt = sc(4)
+    deallocate(mb)
+  end subroutine compmn
 
 end module les_gpu

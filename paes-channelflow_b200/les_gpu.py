@@ -127,6 +127,7 @@ def lib():
         "les_mlp_last_error": (ctypes.c_char_p, [VP]),
         "les_mlp_set_params": (I, [VP, VP, VP]),
         "les_mlp_get_params": (I, [VP, VP, VP]),
+        "les_mlp_set_wait_limit": (I, [VP, ctypes.c_double]),
         "les_mlp_forward": (I, [VP, VP, ctypes.c_longlong, VP, VP]),
         "les_mlp_loss_grad": (I, [VP, VP, VP, ctypes.c_longlong, VP, ctypes.POINTER(D), VP]),
         "les_mlp_adam_step": (I, [VP, VP, VP, ctypes.c_longlong, ctypes.c_float, ctypes.POINTER(D), VP]),
@@ -523,6 +524,11 @@ class Mlp:
         nm = np.zeros(MLP_NNORM, dtype=np.float32)
         self._check(lib().les_mlp_get_params(self.h, p.ctypes.data, nm.ctypes.data))
         return p, nm
+
+    def set_wait_limit(self, seconds):
+        """Limit of each tensor-core MMA wait of this network's kernels
+        (les_mlp_set_wait_limit); default 1 s."""
+        self._check(lib().les_mlp_set_wait_limit(self.h, ctypes.c_double(seconds)))
 
     def forward(self, feat):
         import torch

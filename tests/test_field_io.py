@@ -58,6 +58,7 @@ def test_header_reader_of_the_library(tmp_path, product):
 @pytest.mark.parametrize("rb,background", [(8, False), (8, True), (4, False)])
 def test_gpu_write_then_numpy_read(gpu_lib, product, tmp_path, rb, background):
     cfg = product.channel_config(32, 16, 8, dt=2e-3, re_tau=180.0)
+    cfg.ugal, cfg.vgal = 0.25, -0.125  # the Galilean shift the header must carry
     g = product.LesGpu(cfg)
     g.make_ic(seed=4, amp=0.3, re_tau=180.0)
     for it in range(2):
@@ -71,6 +72,10 @@ def test_gpu_write_then_numpy_read(gpu_lib, product, tmp_path, rb, background):
     h, f = F.read_field(path, real_bytes=rb)
     assert (h["nnx"], h["nny"], h["nnz"]) == (32, 16, 8) and h["time"] == 3.0
     assert h["dt"] == pytest.approx(2e-3, rel=1e-7) and h["utau"] > 0
+    # the post-processing programs' shift formula (calc_pdf.f90:99-100)
+    ugal = (max(0.0, max(h["ugtop"], h["ugbot"])) + min(0.0, min(h["ugtop"], h["ugbot"]))) * 0.5
+    vgal = (max(0.0, max(h["vgtop"], h["vgbot"])) + min(0.0, min(h["vgtop"], h["vgbot"]))) * 0.5
+    assert ugal == pytest.approx(0.25) and vgal == pytest.approx(-0.125)
     for k in "uvwep":
         np.testing.assert_array_equal(f[k], d[k])
     g.close()

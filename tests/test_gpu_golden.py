@@ -1,0 +1,123 @@
+"""FP64 drop-in parity at the benchmark channel configurations, against
+fixtures the oracle wrote on the host (tests/golden/make_channel_golden.py):
+
+  C1: 64^3, Re_tau 180, 100 RK3 steps (snapshots after 10 and 100 steps);
+  C2: 128 x 128 x 96, Re_tau 395, 1000 RK3 steps (after 10, 100 and 1000).
+
+The GPU starts from the oracle's initial field (its checksum is in the
+fixture), steps through les_gpu_step with the fixture's dt and mnout
+cadence, and is compared per snapshot:
+  * the sampled planes of u, v, w, e (field-wise relative error, scale =
+    the field's maximum), the per-level RMS and seeded projections;
+  * compmn's meanbuf rows (mean profile, resolved and SGS moments) and the
+    wall-model scalars;
+  * the u x-spectra at the sampled levels;
+and after every projection the discrete divergence must stay at round-off
+(max |div| below 1e-12 of max|u| nz/zl, the oracle's being ~5e-16).
+
+Tolerances grow with the step count because the two implementations sum in
+different orders and the flow amplifies round-off differences: FP64
+1e-9 after 10 steps, 1e-7 after 100; after 1000 steps of C2 the flow has
+left the laminar start and the fields are compared statistically (mean
+profile and moments) with the bounds below.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import channel_golden as G  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+# field-wise (planes, projections, RMS) and statistics tolerances per snapshot
+TOL_FIELD = {10: 1e-9, 100: 1e-7}
+TOL_STATS = {10: 1e-9, 100: 1e-7}
+# after 1000 steps (C2): the flow is no longer bitwise comparable; the mean
+# profile and the plane RMS values must still agree closely
+TOL_1000 = dict(mean_u=1e-3, rms=2e-2, moments=5e-2)
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _run_case(product, case):
+    fx = dict(np.load(os.path.join(HERE, "golden", case + ".npz")))
+    nx, ny, nz = [int(v) for v in fx["grid"]]
+    re_tau, dt = float(fx["re_tau"]), float(fx["dt"])
+    cfg_o = O.make_config(nx, ny, nz, dt=1e-3, re_tau=re_tau)
+    o = O.Oracle(cfg_o)
+    o.make_ic(seed=int(fx["seed"]), amp=float(fx["amp"]), re_tau=re_tau)
+    f0 = o.get_fields()
+    o.close()
+    for i, k in enumerate("uvwe"):
+        assert abs(f0[k].sum() - fx["ic_sum"][i]) <= 1e-12 * max(abs(fx["ic_sum"][i]), np.abs(f0[k]).sum())
+        assert abs((f0[k] ** 2).sum() - fx["ic_sumsq"][i]) <= 1e-12 * fx["ic_sumsq"][i]
+    g = product.LesGpu(product.channel_config(nx, ny, nz, dt=dt, re_tau=re_tau))
+    g.upload(f0["u"], f0["v"], f0["w"], f0["e"], f0["p"])
+    every = int(fx["mnout_every"])
+    snaps = [int(s) for s in fx["snaps"]]
+    report, div = {}, []
+    for it in range(max(snaps)):
+        g.step(it=it, mnout=(it == 0 or it % every == 0), dt=dt)
+        n = it + 1
+        check_div = n in snaps or n <= 20 or n % 50 == 0
+        if check_div:
+            g.sync()
+            f = g.download()
+            div.append((n, G.divergence_ratio(f, cfg_o.xl, cfg_o.yl, cfg_o.zl)))
+        if n not in snaps:
+            continue
+        fp = G.fingerprint(f)
+        mb, sc = g.stats()
+        r = {}
+        for k in "uvwe":
+            r["plane_" + k] = _rel(fp["plane_" + k], fx["s%d_plane_%s" % (n, k)])
+            r["rms_" + k] = _rel(fp["rms_" + k], fx["s%d_rms_%s" % (n, k)])
+            scale = np.abs(fx["s%d_plane_%s" % (n, k)]).max() * np.sqrt(nx * ny)
+            r["proj_" + k] = float(np.abs(fp["proj_" + k] - fx["s%d_proj_%s" % (n, k)]).max() / scale)
+        mbo = fx["s%d_meanbuf" % n]
+        r["mean_u"] = _rel(mb[3], mbo[3])
+        r["moments"] = max(_rel(mb[i], mbo[i]) for i in (0, 6, 7, 8, 9, 11))
+        r["sgs"] = max(_rel(mb[i], mbo[i]) for i in (13, 14, 15, 16, 17))
+        r["scalars"] = _rel(sc[:2], fx["s%d_scalars" % n][:2])
+        spec = np.array([G.xspectrum(f["u"][z]) for z in G.sample_levels(nz)])
+        r["xspec_u"] = _rel(spec, fx["s%d_xspec_u" % n])
+        report[n] = r
+    g.close()
+    print("\n%s report:" % case)
+    for n, r in report.items():
+        print("  %5d steps: %s" % (n, ", ".join("%s %.2e" % kv for kv in sorted(r.items()))))
+    print("  gpu divergence ratio max %.2e, oracle %.2e" % (max(d for _, d in div), fx["div_ratio"].max()))
+    return fx, report, div
+
+
+def _check(fx, report, div):
+    assert max(d for _, d in div) < 1e-12, div
+    assert fx["div_ratio"].max() < 1e-12
+    for n, r in report.items():
+        if n in TOL_FIELD:
+            tf, ts = TOL_FIELD[n], TOL_STATS[n]
+            for k, v in r.items():
+                tol = tf if k.split("_")[0] in ("plane", "rms", "proj") else ts
+                if k == "xspec_u":
+                    tol = 10 * tf  # quadratic in the field, relative to its maximum
+                assert v < tol, (n, k, v, tol)
+        else:
+            assert r["mean_u"] < TOL_1000["mean_u"], (n, r)
+            assert max(r["rms_" + k] for k in "uvw") < TOL_1000["rms"], (n, r)
+            assert r["moments"] < TOL_1000["moments"], (n, r)
+
+
+def test_c1_hundred_steps_against_fixture(gpu_lib, product):
+    _check(*_run_case(product, "c1"))
+
+
+def test_c2_thousand_steps_against_fixture(gpu_lib, product):
+    _check(*_run_case(product, "c2"))

@@ -188,3 +188,31 @@ def test_learned_features_match_numpy(gpu_lib, product):
         scale = np.abs(ref[:, j]).max()
         err = np.abs(feat[:, j] - ref[:, j]).max()
         assert err <= 1e-6 * scale + 1e-30, (j, err, scale)  # f32 output
+
+
+def test_mma_wait_limit_in_the_learned_stage(gpu_lib, product):
+    """A tensor-core wait that runs out inside the solver's learned stage is
+    reported by les_gpu_sync as LES_ETIMEOUT (the handle's error word is
+    sticky); a new handle on the same context with the limit restored
+    reproduces the stage of a handle that never timed out."""
+    sign = dissipative_sign(product)
+    o, g, m, f = learned_pair(product, sign)
+    m.set_wait_limit(0.0)
+    g.stage(0, True, 1)
+    with pytest.raises(product.LesError) as ei:
+        g.sync()
+    assert ei.value.code == product.LES_ETIMEOUT
+    g.close()
+    m.set_wait_limit(1.0)
+    _, g2, m2, _ = learned_pair(product, sign)
+    g2.stage(0, True, 1)
+    g2.sync()
+    g3 = product.LesGpu(g2.cfg)
+    g3.upload(f["u"], f["v"], f["w"], f["e"], f["p"])
+    g3.set_mlp(m, RE_TAU)
+    g3.set_learned_guard(0.0)
+    g3.stage(0, True, 1)
+    g3.sync()
+    a, b = g2.download(), g3.download()
+    for k in "uvwe":
+        assert np.array_equal(a[k], b[k]), k

@@ -121,3 +121,25 @@ def test_training_reduces_loss(product, mlp):
             first = l
         last = l
     assert last < 0.1 * first, (first, last)
+
+
+def test_mma_wait_limit_runs_out_and_context_stays_usable(product, gpu_lib):
+    """The bounded tensor-core waits: with the limit set to 0 from the host,
+    the training kernel gives up at its first unfinished MMA, drains it
+    (fixed 1 s bound), frees its tensor memory and the host gets
+    LES_ETIMEOUT; with the limit back at 1 s the same call on the same
+    context reproduces the earlier result bit for bit."""
+    m = product.Mlp(O.mlp_init(seed=23))
+    x, t = _inputs(8192, seed=24)
+    f, tt = product.to_feat(x), product.to_target(t)
+    l_ref, g_ref = m.loss_grad(f, tt)
+    m.set_wait_limit(0.0)
+    with pytest.raises(product.LesError) as ei:
+        m.loss_grad(f, tt)
+    assert ei.value.code == product.LES_ETIMEOUT
+    m.set_wait_limit(1.0)
+    l2, g2 = m.loss_grad(f, tt)
+    assert l2 == l_ref and bool((g2 == g_ref).all())
+    with pytest.raises(product.LesError):
+        m.set_wait_limit(-1.0)
+    m.close()

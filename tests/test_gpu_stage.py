@@ -56,6 +56,11 @@ def compare(o, g, tol_f, tol_t, label=""):
     dict(nx=16, ny=16, nz=8, imodel=4, isurface=1, tke_production=1),
     dict(nx=32, ny=16, nz=12, imodel=3, isurface=1, tke_production=1),
     dict(nx=16, ny=32, nz=6, imodel=3, isurface=6, tke_production=1),
+    # the other wall models (lowerbc.f90:126-161, upperbc.f90:124-158)
+    dict(nx=16, ny=16, nz=8, imodel=3, isurface=2, tke_production=0),
+    dict(nx=32, ny=16, nz=8, imodel=3, isurface=3, tke_production=0),
+    dict(nx=16, ny=16, nz=8, imodel=3, isurface=4, tke_production=1),
+    dict(nx=16, ny=32, nz=8, imodel=4, isurface=5, tke_production=0),
 ], ids=lambda c: "{nx}x{ny}x{nz}-m{imodel}-s{isurface}-p{tke_production}".format(**c))
 def test_one_stage_then_two_steps_fp64(gpu_lib, product, case):
     kw = dict(case)

@@ -122,6 +122,11 @@ CASES = [
     dict(nx=16, ny=16, nz=8, imodel=3, isurface=6, prod=0),
     dict(nx=16, ny=16, nz=8, imodel=4, isurface=1, prod=1),
     dict(nx=24, ny=16, nz=12, imodel=3, isurface=1, prod=1),
+    # the other wall models of lowerbc.f90:126-161 / upperbc.f90:124-158
+    dict(nx=16, ny=16, nz=8, imodel=3, isurface=2, prod=0),
+    dict(nx=16, ny=16, nz=8, imodel=3, isurface=3, prod=0),
+    dict(nx=16, ny=16, nz=8, imodel=3, isurface=4, prod=1),
+    dict(nx=16, ny=16, nz=8, imodel=4, isurface=5, prod=0),
 ]
 
 
