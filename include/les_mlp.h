@@ -7,14 +7,21 @@
  * (tau_ij = -2 nu_t S_ij) with tau_ij predicted from the local resolved
  * velocity gradients.  The solver uses it when its configuration has
  * imodel = LES_SGS_LEARNED (les_gpu.h) and a network is attached with
- * les_gpu_set_mlp; stages whose plane-averaged dissipation
- * -<tau_ij S_ij> comes out negative fall back to the Deardorff stresses.
+ * les_gpu_set_mlp; stages whose mean dissipation -<tau_ij S_ij> comes out
+ * negative, or (les_gpu_set_learned_guard) outside a factor of the
+ * Smagorinsky estimate, fall back to the Deardorff stresses.
  *
  * Network: 11 -> 64 -> 64 -> 64 -> 6, GELU (tanh form) after the hidden
- * layers, bf16 weights and activations, f32 accumulation.
- *   inputs  f = (ux, vx, wx, uy, vy, wy, uz, vz, wz) * Delta, z+, Delta
- *           normalised as x_j = (f_j - in_shift_j) * in_scale_j
- *   outputs y -> tau = y * out_scale + out_shift for
+ * layers, bf16 weights and activations, f32 accumulation.  The closure is
+ * dimensionless, so that one network serves every grid and filter width
+ * Delta = (dx dy dz)^(1/3):
+ *   inputs  x = (ux, vx, wx, uy, vy, wy, uz, vz, wz) / |G|  (|G| the
+ *           Frobenius norm of the nine resolved gradients at the cell
+ *           centre), min(z_w / Delta, 16), z_w / h  (z_w the distance to the
+ *           nearest wall, h = zl / 2), normalised as
+ *           x_j' = (x_j - in_shift_j) * in_scale_j
+ *   outputs y -> c = y * out_scale + out_shift and
+ *           tau_ij = (Delta |G|)^2 c_ij for
  *           (tau11, tau22, tau33, tau12, tau13, tau23)
  * Parameters (LES_MLP_NPARAM floats, this order):
  *   W1[64][11], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], W4[6][64], b4[6]
@@ -38,8 +45,9 @@ extern "C" {
 #define LES_MLP_NOUT   6
 #define LES_MLP_NPARAM 9478
 #define LES_MLP_NNORM  34
-/* Sample layouts on the device: features bf16 [n][16] (normalised, columns
- * 11..15 zero), outputs and targets f32 [n][8] (columns 6, 7 unused). */
+/* Sample layouts on the device: features bf16 [n][16] (normalised inputs in
+ * columns 0..10; the network ignores 11..15), outputs and targets f32 [n][8]
+ * (columns 6, 7 unused). */
 #define LES_MLP_FEAT_STRIDE 16
 #define LES_MLP_OUT_STRIDE  8
 
@@ -82,8 +90,10 @@ int les_mlp_adam_step(les_mlp* m, const void* feat, const float* target, long lo
                       void* stream);
 
 /* Attach (or with m == NULL detach) a network to a solver handle whose
- * configuration has imodel = LES_SGS_LEARNED.  re_tau sets the z+ feature.
- * The handle keeps a reference to m: destroy the handle first. */
+ * configuration has imodel = LES_SGS_LEARNED.  re_tau (> 0) is the run's
+ * friction Reynolds number, recorded with the network; the features do not
+ * depend on it.  Resets the stage counters of les_gpu_learned_counts.  The
+ * handle keeps a reference to m: destroy the handle first. */
 int les_gpu_set_mlp(les_handle* h, les_mlp* m, double re_tau);
 
 /* After a synchronising call: 1 if the last stage used the network (0 if
@@ -92,17 +102,21 @@ int les_gpu_set_mlp(les_handle* h, les_mlp* m, double re_tau);
 int les_gpu_learned_status(les_handle* h, int* used, double* dissipation);
 
 /* The fallback test of each stage: the network is used when its mean
- * dissipation is >= 0 (the spec'd test) and, with ratio > 0, within a factor
- * ratio of the Deardorff model's mean dissipation 2 <nu_t S_ij S_ij> on the
- * same state (nu_t = min(0.1 Delta sqrt(e), xkmax) + nu, e at the cell
- * centre).  The second test keeps a network out of states it was not
- * trained for (a network trained on one grid imposes that grid's stress
- * levels on another).  Default ratio 4; ratio <= 0 disables it.  Drops the
- * handle's captured step graphs. */
+ * dissipation -<tau_ij S_ij> is >= 0 (the spec'd test) and, with
+ * ratio > 0, within a factor ratio of the reference dissipation
+ * <(0.1 Delta)^2 |S|^3>, the Smagorinsky estimate with the constant of the
+ * reference's imodel 4 (complen.f90:22-23), |S| = (2 S_ij S_ij)^(1/2), on
+ * the same state.  The second test keeps a network out of states whose
+ * sub-filter dissipation it would misjudge by more than that factor.
+ * Default ratio 4; ratio <= 0 disables it.  Drops the handle's captured
+ * step graphs. */
 int les_gpu_set_learned_guard(les_handle* h, double ratio);
-/* After a synchronising call: the Deardorff mean dissipation of the last
- * learned stage (the reference value of the second test). */
-int les_gpu_learned_deardorff(les_handle* h, double* dissipation);
+/* After a synchronising call: the reference (Smagorinsky) mean dissipation
+ * of the last learned stage. */
+int les_gpu_learned_reference(les_handle* h, double* dissipation);
+/* Stages evaluated with the network attached since les_gpu_set_mlp, and
+ * how many of them used it (synchronising). */
+int les_gpu_learned_counts(les_handle* h, long long* stages, long long* used);
 
 /* Training data (synchronous; out pointers are device memory).
  *
@@ -115,14 +129,16 @@ int les_gpu_learned_deardorff(les_handle* h, double* dissipation);
  * tau_ij = filt(u_i u_j) - filt(u_i) filt(u_j) (w averaged to the centres);
  * with_model != 0 adds the filtered Deardorff stress of the fine run,
  * -2 nu_t S_ij with nu_t = 0.1 dsl sqrt(e) at the fine cell centres, so
- * tau_ij is the total sub-filter stress the coarse grid misses.
+ * tau_ij is the total sub-filter stress the coarse grid misses.  fz is 1 or
+ * even; w at the coarse faces is the z box of fz fine cells centred on the
+ * face (trapezoid weights).
  *
  * les_gpu_learned_features: the network's raw inputs at every cell centre
- * of the current state, f32 [nnx*nny*nnz][16] (columns 0..10 as in the
- * feature list above, unnormalised; 11..15 zero), computed by the kernels
- * the learned stage uses. */
+ * of the current state, f32 [nnx*nny*nnz][16]: columns 0..10 the inputs x
+ * above, unnormalised; column 11 Delta |G|; 12..15 zero.  Computed by the
+ * kernels the learned stage uses. */
 int les_gpu_learn_filter(les_handle* h, int fxy, int fz, int with_model, double* out);
-int les_gpu_learned_features(les_handle* h, double re_tau, float* feat);
+int les_gpu_learned_features(les_handle* h, float* feat);
 
 #ifdef __cplusplus
 }

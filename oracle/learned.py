@@ -4,7 +4,9 @@ closure's grid operations, independent of the C++ oracle's Stockham DFT.
 - features(): the network inputs at the cell centres of a state (the
   gradient stencils of the learned stage: spectral x/y derivatives, w
   averaged to the centres, centred z differences of u, v that are
-  one-sided at the walls as derivs1.f90 / derivs2.f90 set the wall rows);
+  one-sided at the walls as derivs1.f90 / derivs2.f90 set the wall rows),
+  made dimensionless: g / |G|, min(z_w / Delta, 16), z_w / h, with the
+  output scale Delta |G| (tau = (Delta |G|)^2 c);
 - divergence(): the dealiased stress divergence added to ru, rv, rw;
 - filter_fields(): the explicit filter that makes training data from a
   fine run (z box average, x-y box-filter transfer with truncation to the
@@ -85,20 +87,28 @@ def gradients(u, v, w, xl, yl, zl):
     return g
 
 
-def features(u, v, w, xl, yl, zl, re_tau):
-    """Raw network inputs (nz*ny*nx, 11): gradients * Delta, z+, Delta."""
+ZW_CAP = 16.0
+
+
+def features(u, v, w, xl, yl, zl):
+    """Raw network inputs (nz*ny*nx, 11) and the output scale Delta |G|
+    (nz*ny*nx,): inputs g_j / |G| (the nine gradients over their Frobenius
+    norm), min(z_w / Delta, 16), z_w / h (z_w the distance to the nearest
+    wall, h = zl / 2)."""
     nz, ny, nx = u.shape
     dz = zl / nz
     dsl = (xl / nx * yl / ny * dz) ** (1.0 / 3.0)
     g = gradients(u, v, w, xl, yl, zl)
+    gm = np.sqrt((g ** 2).sum(axis=0))
+    rg = np.where(gm > 0, 1.0 / np.where(gm > 0, gm, 1.0), 0.0)
     zc = (np.arange(nz) + 0.5) * dz
-    zp = np.minimum(zc, zl - zc) * re_tau / (zl / 2)
+    zw = np.minimum(zc, zl - zc)
     f = np.zeros((nz, ny, nx, 11))
     for j in range(9):
-        f[..., j] = g[j] * dsl
-    f[..., 9] = zp[:, None, None]
-    f[..., 10] = dsl
-    return f.reshape(-1, 11)
+        f[..., j] = g[j] * rg
+    f[..., 9] = np.minimum(zw / dsl, ZW_CAP)[:, None, None]
+    f[..., 10] = (zw / (zl / 2))[:, None, None]
+    return f.reshape(-1, 11), (gm * dsl).reshape(-1)
 
 
 def dissipation(g, tau):
@@ -110,25 +120,21 @@ def dissipation(g, tau):
     return float(d.mean())
 
 
-def deardorff_dissipation(g, e, dsl, xkmax, nu=0.0):
-    """Mean of 2 nu_t S_ij S_ij over all cell centres, nu_t = min(0.1 dsl
-    sqrt(e_c), xkmax) + nu with e_c = (e(k-1) + e(k)) / 2 and e(0) read as
-    e(1); e (nz, ny, nx) on the w-levels 1..nz."""
+def reference_dissipation(g, dsl):
+    """Mean of (0.1 dsl)^2 |S|^3 over all cell centres, |S|^2 = 2 S_ij S_ij:
+    the Smagorinsky estimate with the constant of complen.f90:22-23."""
     s11, s22, s33 = g[0], g[4], g[8]
     s12, s13, s23 = 0.5 * (g[3] + g[1]), 0.5 * (g[6] + g[2]), 0.5 * (g[7] + g[5])
-    em = np.concatenate([e[:1], e[:-1]], axis=0)
-    ec = 0.5 * (em + e)
-    nut = np.minimum(0.1 * dsl * np.sqrt(np.maximum(ec, 0.0)), xkmax) + nu
-    ss = s11 ** 2 + s22 ** 2 + s33 ** 2 + 2 * (s12 ** 2 + s13 ** 2 + s23 ** 2)
-    return float((2 * nut * ss).mean())
+    ss = 2 * (s11 ** 2 + s22 ** 2 + s33 ** 2 + 2 * (s12 ** 2 + s13 ** 2 + s23 ** 2))
+    return float((0.01 * dsl * dsl * ss * np.sqrt(ss)).mean())
 
 
-def network_used(dis, dis_d, guard):
+def network_used(dis, dis_r, guard):
     """The stage's fallback rule: the network's mean dissipation must be
-    >= 0 and, with guard > 0, within a factor guard of Deardorff's."""
+    >= 0 and, with guard > 0, within a factor guard of the reference's."""
     if not dis >= 0:
         return 0
-    if guard > 0 and not (dis_d > 0 and dis <= guard * dis_d and guard * dis >= dis_d):
+    if guard > 0 and not (dis_r > 0 and dis <= guard * dis_r and guard * dis >= dis_r):
         return 0
     return 1
 
@@ -228,11 +234,15 @@ def filter_fields(u, v, w, xl, yl, fxy, fz, tau_model=None):
         for i in range(6):
             q[3 + i] = q[3 + i] + tau_model[i]
     qz = [a.reshape(nzc, fz, ny, nx).mean(axis=1) for a in q]
-    if fz == 2:
-        wst = np.stack([0.25 * _wl(w, 2 * K - 1, nz) + 0.5 * _wl(w, 2 * K, nz) + 0.25 * _wl(w, 2 * K + 1, nz)
-                        for K in range(1, nzc + 1)])
-    else:
+    if fz == 1:
         wst = np.stack([_wl(w, K, nz) for K in range(1, nzc + 1)])
+    else:
+        # the box of fz fine cells centred on coarse face K by the trapezoid
+        # rule: weights 1/(2 fz) on faces fz K -/+ fz/2, 1/fz between
+        h = fz // 2
+        wst = np.stack([(0.5 * (_wl(w, fz * K - h, nz) + _wl(w, fz * K + h, nz)) +
+                         sum(_wl(w, j, nz) for j in range(fz * K - h + 1, fz * K + h))) / fz
+                        for K in range(1, nzc + 1)])
     qz.append(wst)
     Q = np.array([[_filter_xy(a[K], nxc, nyc, xl, yl) for K in range(nzc)] for a in qz])
     out = np.zeros((9, nzc, nyc, nxc))

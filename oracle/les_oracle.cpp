@@ -348,10 +348,11 @@ struct Les {
   int learned_used = 0;
   double learned_dissip = 0.0;
   // second fallback test: the network's mean dissipation must lie within a
-  // factor `learned_guard` of the Deardorff model's on the same state
-  // (learned_guard <= 0: only the sign test)
+  // factor `learned_guard` of the reference (Smagorinsky) dissipation on the
+  // same state (learned_guard <= 0: only the sign test)
   double learned_guard = 4.0;
-  double learned_dissip_d = 0.0;
+  double learned_dissip_r = 0.0;
+  long long learned_stages = 0, learned_stages_used = 0;
   T sgs_mom = (T)1;  // weight of the interior momentum stresses of compsgs1
   Levels<T> lru, lrv, lrw;
 
@@ -763,12 +764,13 @@ struct Les {
   //   ux.. = spectral x/y derivatives; wx, wy of (w(k) + w(k-1))/2;
   //   wz = (w(k) - w(k-1))/dz; uz, vz = centred (u(k+1) - u(k-1))/(2dz),
   //   one-sided at k = 1 and nnz (derivs1.f90 / derivs2.f90 wall rows);
-  // features (g * dsl, z+, dsl), normalised, through the FP64 network; the
-  // stage uses the network when the mean of -tau_ij S_ij is >= 0 and, with
-  // learned_guard > 0, within a factor learned_guard of the Deardorff mean
-  // dissipation 2 nu_t S_ij S_ij (nu_t = min(0.1 dsl sqrt(e_c), xkmax) + nu,
-  // e_c = (e(k-1) + e(k)) / 2 with e(0) read as e(1)), and then adds the
-  // dealiased stress divergence to ru, rv, rw:
+  // dimensionless features (g / |G|, min(z_w / dsl, 16), z_w / h),
+  // normalised, through the FP64 network; tau = (dsl |G|)^2 c with c the
+  // de-normalised outputs; the stage uses the network when the mean of
+  // -tau_ij S_ij is >= 0 and, with learned_guard > 0, within a factor
+  // learned_guard of the reference mean dissipation (0.1 dsl)^2 |S|^3
+  // (|S|^2 = 2 S_ij S_ij; the Smagorinsky estimate with complen.f90:22-23's
+  // constant), and then adds the dealiased stress divergence to ru, rv, rw:
   //   ru += -d/dx tau11 - d/dy tau12 - (tau13w(k) - tau13w(k-1))/dz, ...
   // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on the interior w-levels and 0
   // on the walls (the wall model's stresses stay in compsgs1), plus the
@@ -780,8 +782,7 @@ struct Les {
     std::vector<std::vector<T>> g(9, std::vector<T>(ps));
     std::vector<T> wc(ps);
     const double h = (double)zl / 2.0;
-    double dsum_ = 0.0, dsumd_ = 0.0;
-    const double nu_mol = (double)cfg.nu;
+    double dsum_ = 0.0, dsumr_ = 0.0;
     std::vector<double> nuA((size_t)NZ + 2, 0.0), nuB((size_t)NZ + 2, 0.0);
     for (int iz = 1; iz <= NZ; iz++) {
       sp.xderiv(u.at(iz), g[0].data(), xk.data(), nnx, nny);
@@ -805,35 +806,41 @@ struct Les {
       const double zc = ((double)iz - 0.5) * (double)dz;
       const double zw = std::min(zc, (double)zl - zc);
       MlpTrace tr;
+      const double zd = std::min(zw / (double)dsl, 16.0);
       for (size_t q = 0; q < ps; q++) {
         double f[kIn], x[kIn];
-        for (int jj = 0; jj < 9; jj++) f[jj] = (double)(g[jj][q] * dsl);
-        f[9] = zw * re_tau / h;
-        f[10] = (double)dsl;
+        double g2 = 0.0;
+        for (int jj = 0; jj < 9; jj++) g2 += (double)g[jj][q] * (double)g[jj][q];
+        const double gm = std::sqrt(g2), rg = gm > 0.0 ? 1.0 / gm : 0.0;
+        for (int jj = 0; jj < 9; jj++) f[jj] = (double)g[jj][q] * rg;
+        f[9] = zd;
+        f[10] = zw / h;
         for (int jj = 0; jj < kIn; jj++) x[jj] = (f[jj] - mlpN[jj]) * mlpN[kIn + jj];
         mlp_forward(mlpP.data(), x, tr, mlp_bf16);
+        const double sc = gm * (double)dsl, sc2 = sc * sc;
         double t[kOut];
         for (int o = 0; o < kOut; o++) {
-          t[o] = tr.y[o] * mlpN[2 * kIn + o] + mlpN[2 * kIn + kOut + o];
+          t[o] = sc2 * (tr.y[o] * mlpN[2 * kIn + o] + mlpN[2 * kIn + kOut + o]);
           TA(o, iz)[q] = (T)t[o];
         }
         const double s11 = g[0][q], s22 = g[4][q], s33 = g[8][q];
         const double s12 = 0.5 * ((double)g[3][q] + g[1][q]), s13 = 0.5 * ((double)g[6][q] + g[2][q]),
                      s23 = 0.5 * ((double)g[7][q] + g[5][q]);
         dsum_ += -(t[0] * s11 + t[1] * s22 + t[2] * s33 + 2.0 * (t[3] * s12 + t[4] * s13 + t[5] * s23));
-        const double ec = 0.5 * ((double)e.at(iz > 1 ? iz - 1 : 1)[q] + (double)e.at(iz)[q]);
-        const double nut = std::min(0.1 * (double)dsl * std::sqrt(std::max(ec, 0.0)), (double)xkmax) + nu_mol;
-        dsumd_ += 2.0 * nut * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23));
+        const double ss = 2.0 * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23));
+        dsumr_ += 0.01 * (double)dsl * (double)dsl * ss * std::sqrt(ss);
         nuA[iz] += t[4] * (double)g[6][q] + t[5] * (double)g[7][q];
         nuB[iz] += (double)g[6][q] * g[6][q] + (double)g[7][q] * g[7][q];
       }
     }
     learned_dissip = dsum_ / ((double)ps * NZ);
-    learned_dissip_d = dsumd_ / ((double)ps * NZ);
+    learned_dissip_r = dsumr_ / ((double)ps * NZ);
     learned_used = learned_dissip >= 0.0 ? 1 : 0;  // NaN -> fallback
-    if (learned_guard > 0.0 && !(learned_dissip_d > 0.0 && learned_dissip <= learned_guard * learned_dissip_d &&
-                                 learned_guard * learned_dissip >= learned_dissip_d))
+    if (learned_guard > 0.0 && !(learned_dissip_r > 0.0 && learned_dissip <= learned_guard * learned_dissip_r &&
+                                 learned_guard * learned_dissip >= learned_dissip_r))
       learned_used = 0;
+    learned_stages++;
+    learned_stages_used += learned_used;
     if (!learned_used) return;
     // stress divergence
     std::vector<T> t13w_m(ps), t13w_p(ps), t23w_m(ps), t23w_p(ps), f1(ps), f2(ps);
@@ -1307,11 +1314,11 @@ void orc_learned_status(void* hp, int* used, double* dissipation) {
   OrcHandle* h = (OrcHandle*)hp;
   DISPATCH(h, { if (used) *used = L.learned_used; if (dissipation) *dissipation = L.learned_dissip; });
 }
-// Deardorff mean dissipation of the last learned stage.
-double orc_learned_deardorff(void* hp) {
+// Reference (Smagorinsky) mean dissipation of the last learned stage.
+double orc_learned_reference(void* hp) {
   OrcHandle* h = (OrcHandle*)hp;
   double d = 0.0;
-  DISPATCH(h, { d = L.learned_dissip_d; });
+  DISPATCH(h, { d = L.learned_dissip_r; });
   return d;
 }
 // Factor of the dissipation test (<= 0: sign test only).

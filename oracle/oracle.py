@@ -114,8 +114,8 @@ def lib():
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int]
         L.orc_set_mlp.argtypes = [P, D, D, ctypes.c_double, ctypes.c_int]
         L.orc_learned_status.argtypes = [P, ctypes.POINTER(ctypes.c_int), D]
-        L.orc_learned_deardorff.argtypes = [P]
-        L.orc_learned_deardorff.restype = ctypes.c_double
+        L.orc_learned_reference.argtypes = [P]
+        L.orc_learned_reference.restype = ctypes.c_double
         L.orc_set_learned_guard.argtypes = [P, ctypes.c_double]
         L.orc_get_learned.argtypes = [P, D, D, D]
         L.orc_bf16_round.restype = ctypes.c_double
@@ -220,9 +220,9 @@ class Oracle:
         lib().orc_learned_status(self.h, ctypes.byref(used), _ptr(d))
         return used.value, float(d[0])
 
-    def learned_deardorff(self):
-        """Deardorff mean dissipation of the last learned stage."""
-        return float(lib().orc_learned_deardorff(self.h))
+    def learned_reference(self):
+        """Reference (Smagorinsky) mean dissipation of the last learned stage."""
+        return float(lib().orc_learned_reference(self.h))
 
     def set_learned_guard(self, ratio):
         """Factor of the dissipation test against Deardorff (<= 0: off)."""

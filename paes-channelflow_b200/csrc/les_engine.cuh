@@ -169,7 +169,9 @@ struct EngineBase {
   // factor of the fallback test against the Deardorff dissipation (<= 0:
   // the sign test only) and the Deardorff mean dissipation of the last stage
   virtual void set_learned_guard(double ratio) = 0;
-  virtual double learned_deardorff() = 0;
+  virtual double learned_reference() = 0;
+  // stages evaluated since the network was attached, and those that used it
+  virtual void learned_counts(long long* stages, long long* used) = 0;
   virtual void learned_features(double re_tau, float* feat) = 0;
   virtual void learn_filter(int fxy, int fz, int with_model, double* out) = 0;
   // this state := the state of `src` regridded onto this grid (redim.f90)
@@ -215,9 +217,9 @@ struct Engine : EngineBase {
   DevBuf<T> ltau;      // [8][NZ][NY][NX] tau at the cell centres + viscosity products
   DevBuf<uint4> lfeat; // [N][16] bf16 features
   DevBuf<float> fraw;  // [N][16] raw f32 features (training data)
-  DevBuf<double> lpart, lstat, lnut, lpartd;
+  DevBuf<double> lpart, lstat, lnut;
+  DevBuf<unsigned long long> lcount;  // [stages, stages that used the network]
   double lguard = 4.0;
-  static constexpr int kDdBlocks = 4;  // blocks per level of k_deardorff_dissip (partial sums 4 * NZ)
   DevBuf<int> lflag;
   DevBuf<T> fscr, fcp;      // filter scratch: z-averaged fine planes, coarse planes
   DevBuf<cx<T>> fsh, fch;   // filter scratch: fine and coarse spectra
@@ -498,15 +500,18 @@ struct Engine : EngineBase {
     lgy.alloc(6 * nm * NZ);
     ltau.alloc(8 * ps * NZ);
     lfeat.alloc(2 * ps * NZ);
-    lpart.alloc((size_t)nsm * kInferCtasPerSm);
+    lpart.alloc((size_t)2 * nsm * kInferCtasPerSm);  // per-CTA pairs: network, reference
     lnut.alloc((size_t)NZ * kNuChunks * 2 + NZ + 1);  // partial sums, then the face values
     lstat.alloc(3);
-    lpartd.alloc((size_t)kDdBlocks * NZ);
+    lcount.alloc(2);
     lflag.alloc(1);
   }
   void set_mlp(const MlpDev* p, double rt) override {
     if (p && cfg.imodel != LES_SGS_LEARNED) throw std::invalid_argument("the handle's imodel is not LES_SGS_LEARNED");
-    if (p) learned_alloc();
+    if (p) {
+      learned_alloc();
+      LES_CUDA(cudaMemsetAsync(lcount.p, 0, 2 * sizeof(unsigned long long), st));
+    }
     mlp = p;
     re_tau = rt;
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);  // captured with the previous closure
@@ -518,13 +523,22 @@ struct Engine : EngineBase {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);  // captured with the previous factor
     graphs.clear();
   }
-  double learned_deardorff() override {
+  double learned_reference() override {
     double v[3] = {0.0, 0.0, 0.0};
     if (learned_on()) {
       LES_CUDA(cudaMemcpyAsync(v, lstat.p, sizeof(v), cudaMemcpyDeviceToHost, st));
       LES_CUDA(cudaStreamSynchronize(st));
     }
     return v[2];
+  }
+  void learned_counts(long long* stages, long long* used) override {
+    unsigned long long v[2] = {0ull, 0ull};
+    if (learned_on()) {
+      LES_CUDA(cudaMemcpyAsync(v, lcount.p, sizeof(v), cudaMemcpyDeviceToHost, st));
+      LES_CUDA(cudaStreamSynchronize(st));
+    }
+    if (stages) *stages = (long long)v[0];
+    if (used) *used = (long long)v[1];
   }
   void learned_status(int* used, double* dissipation) override {
     double v[2] = {0.0, 0.0};
@@ -537,24 +551,24 @@ struct Engine : EngineBase {
   }
   // y-inverse rows of the velocity spectra, then gradients and features
   // at the cell centres (bf16 normalised by the attached network, or raw f32)
-  void learned_features_into(void* feat, bool raw, double rt) {
+  void learned_features_into(void* feat, bool raw) {
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = ColCfg<NN, T>;
       launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC / 2), NZ, 3), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
              (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)ky0, tw);
     });
-    const T zpl = (T)(rt / (cfg.zl / 2.0));
+    const T inv_h = (T)(2.0 / cfg.zl);
     with_small(NX, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using L = LgxCfg<NN>;
       const unsigned grid = cdiv((size_t)NZ * NY, L::RB);
       if (raw)
         launch(k_lgrad_x<T, NN, true>, dim3(grid), dim3(L::THREADS), L::template smem<T>(), st, (const cx<T>*)lgy.p,
-               feat, mlp, NY, NZ, (T)kx0, (T)dzm, (T)dsl, (T)dz, (T)cfg.zl, zpl, tw);
+               feat, mlp, NY, NZ, (T)kx0, (T)dzm, (T)dsl, (T)dz, (T)cfg.zl, inv_h, tw);
       else
         launch(k_lgrad_x<T, NN, false>, dim3(grid), dim3(L::THREADS), L::template smem<T>(), st, (const cx<T>*)lgy.p,
-               feat, mlp, NY, NZ, (T)kx0, (T)dzm, (T)dsl, (T)dz, (T)cfg.zl, zpl, tw);
+               feat, mlp, NY, NZ, (T)kx0, (T)dzm, (T)dsl, (T)dz, (T)cfg.zl, inv_h, tw);
     });
   }
   // raw (unnormalised) features of the current state, f32 [N][16]
@@ -619,12 +633,13 @@ struct Engine : EngineBase {
   void learned_features(double rt, float* feat) override {
     if (phase != 0) throw std::logic_error("learned_features inside a split comp1..comp2 sequence");
     learned_alloc();
-    learned_features_into(feat, true, rt);
+    (void)rt;  // the features do not depend on Re_tau
+    learned_features_into(feat, true);
   }
   // explicit filter of the current state onto the grid (NX/fxy, NY/fxy, NZ/fz)
   void learn_filter(int fxy, int fz, int with_model, double* out) override {
     if (phase != 0) throw std::logic_error("learn_filter inside a split comp1..comp2 sequence");
-    if (fxy < 1 || fz < 1 || fz > 2 || NX % fxy || NY % fxy || NZ % fz)
+    if (fxy < 1 || fz < 1 || (fz > 1 && fz % 2) || NX % fxy || NY % fxy || NZ % fz)
       throw std::invalid_argument("learn_filter: unsupported filter factors for this grid");
     const int NXc = NX / fxy, NYc = NY / fxy, NZc = NZ / fz, KXc = NXc / 2;
     if (!supported_small(NXc) || !supported_small(NYc) || NZc < 4)
@@ -637,7 +652,7 @@ struct Engine : EngineBase {
     if (with_model) {
       learned_alloc();
       if (fraw.n < 16 * ps * NZ) { fraw.release(); fraw.alloc(16 * ps * NZ); }
-      learned_features_into(fraw.p, true, 1.0);  // the gradients (columns 0..8) do not depend on re_tau
+      learned_features_into(fraw.p, true);
     }
     to_physical(uh.p, phys[0].p, NZ);
     to_physical(vh.p, phys[1].p, NZ);
@@ -676,16 +691,14 @@ struct Engine : EngineBase {
   // gradients -> features -> network -> tau and the fallback flag
   void learned_pre(const StageArgs& a) {
     const size_t N = ps * NZ;
-    learned_features_into(lfeat.p, false, re_tau);
+    learned_features_into(lfeat.p, false);
     const long long ntiles = ((long long)N + 127) / 128;
     const int grid = (int)std::min<long long>((ntiles + kInferGroups - 1) / kInferGroups, (long long)nsm * kInferCtasPerSm);
     MlpOutTau<T> out{ltau.p, (long long)N};
     launch(k_mlp_infer<MlpOutTau<T>>, dim3(grid), dim3(128 * kInferGroups), kInferSmem, st, mlp,
            (const uint4*)lfeat.p, (long long)N, out, lpart.p, err.p);
-    launch(k_deardorff_dissip<T>, dim3(kDdBlocks, NZ), dim3(256), 0, st, (const uint4*)lfeat.p, (const T*)(e.p + ps),
-           mlp, (int)ps, (T)(0.1 * dsl), (T)a.xkmax, (T)a.nu, (T)(1.0 / dsl), lpartd.p);
-    launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, (const double*)lpartd.p,
-           kDdBlocks * NZ, 1.0 / ((double)N * dsl), lguard, lflag.p, lstat.p);
+    launch(k_learned_flag, dim3(1), dim3(32), 0, st, (const double*)lpart.p, grid, 1.0 / ((double)N * dsl), lguard,
+           lflag.p, lstat.p, lcount.p);
   }
   // tau^ and its divergence into the new tendencies (th reuses lgy)
   void learned_post(const StageArgs& a) {

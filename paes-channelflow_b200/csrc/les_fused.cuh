@@ -10,6 +10,9 @@
 // transform per phase:
 //   phase I   (inverse)  w0: U+iV (z+1)   w1: W+iE (z+1)   w2: UX+iVX (z)
 //                        w3: UY+iVY (z)   w4: WX+iWY (z)   w5: EX+iEY (le)
+//             (when the learned closure supplies the interior momentum
+//             stresses only ux and vy are needed, for the divergence
+//             diagnostic: w2 transforms UX+iVY, w3 and w4 idle)
 //   phase II  (pointwise, all threads) the eleven flux rows of k_flux
 //   phase III (forward)  w0: A+iPu  w1: B+iPv  w2: C+iG  w3: D+iPw
 //                        w4: F+iPe  w5: H
@@ -262,7 +265,8 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
   const WallParams& wp = *f.wp;
   // weight of the interior momentum stresses: 0 when the learned closure
   // supplies them (the wall rows stay)
-  const T mom = (f.lflag && f.lflag[0]) ? (T)0 : (T)1;
+  const bool learned = (f.lflag && f.lflag[0]);
+  const T mom = learned ? (T)0 : (T)1;
 
   auto mixrow = [&](int j, int z) -> const cx<T>* {
     return reinterpret_cast<const cx<T>*>(f.in.p[j]) + ((size_t)(z - 1) * MY + y) * KX;
@@ -310,7 +314,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
       if (warp == 1) { dst = WEs(sm1); A = mixrow(4, zm); B = mixrow(6, min(zm, NZ - 1)); ce = true; }
       if (warp == 2) { dst = UVs(s0); A = mixrow(0, z0); B = mixrow(2, z0); }
       if (warp == 3) { dst = WEs(s0); A = z0 < NZ ? mixrow(4, z0) : nullptr; B = mixrow(6, min(z0, NZ - 1)); ce = true; }
-      if (warp == 4) { dst = work[0]; A = mixrow(4, zm); ma = true; B = mixrow(5, zm); }  // WX + iWY at z0-1
+      if (warp == 4 && !learned) { dst = work[0]; A = mixrow(4, zm); ma = true; B = mixrow(5, zm); }  // WX + iWY at z0-1
     }
     if (dst) {
       inv(dst, A, ma, B, mb);
@@ -327,10 +331,12 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
       wall_stress<T>(wp.w[0], wp, a, 0, uv.x, uv.y, tu, tv);
       carry[x] = mk(tu, tv);
     }
+  } else if (learned) {
+    for (int x = threadIdx.x; x < MX; x += blockDim.x) carry[x] = zero_cx<T>();
   } else {
     for (int x = threadIdx.x; x < MX; x += blockDim.x) {
       cx<T> uvm = UVs(sm1)[S(x)], uv0 = UVs(s0)[S(x)], wxy = work[0][S(x)];
-      T xk = mom * xkk(WEs(sm1)[S(x)].y);
+      T xk = xkk(WEs(sm1)[S(x)].y);
       T uz = (uv0.x - uvm.x) * dzm, vz = (uv0.y - uvm.y) * dzm;
       carry[x] = mk(-xk * (uz + wxy.x), -xk * (vz + wxy.y));
     }
@@ -358,9 +364,13 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
           B = mixrow(6, min(z + 1, NZ - 1));
           ce = true;
           break;
-        case 2: dst = work[0]; A = mixrow(0, z); B = mixrow(2, z); ma = mb = true; break;  // UX + iVX
-        case 3: dst = work[1]; A = mixrow(1, z); B = mixrow(3, z); break;                 // UY + iVY
-        case 4:                                                                           // WX + iWY
+        case 2:
+          if (learned) { dst = work[0]; A = mixrow(0, z); ma = true; B = mixrow(3, z); }  // UX + iVY
+          else { dst = work[0]; A = mixrow(0, z); B = mixrow(2, z); ma = mb = true; }     // UX + iVX
+          break;
+        case 3: if (!learned) { dst = work[1]; A = mixrow(1, z); B = mixrow(3, z); } break;  // UY + iVY
+        case 4:                                                                              // WX + iWY
+          if (learned) break;
           dst = work[2];
           if (z <= NZ - 1) { A = mixrow(4, z); ma = true; B = mixrow(5, z); } else zero = true;
           break;
@@ -389,7 +399,11 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
     for (int x = threadIdx.x; x < MX; x += blockDim.x) {
       const cx<T> uvm = UVs(sm1)[S(x)], uv0 = UVs(s0)[S(x)], uv1 = UVs(sp1)[S(x)];
       const cx<T> wem = WEs(sm1)[S(x)], we0 = WEs(s0)[S(x)], we1 = WEs(sp1)[S(x)];
-      const cx<T> dxv = work[0][S(x)], dyv = work[1][S(x)], wxy = work[2][S(x)];
+      // learned: work[0] holds (ux, vy); the other gradients are not needed
+      const cx<T> w0 = work[0][S(x)];
+      const cx<T> dxv = learned ? mk(w0.x, (T)0) : w0;
+      const cx<T> dyv = learned ? mk((T)0, w0.y) : work[1][S(x)];
+      const cx<T> wxy = learned ? zero_cx<T>() : work[2][S(x)];
       cx<T> exy = top ? zero_cx<T>() : work[3][S(x)];
       if (clip) { exy.x += dEX[x]; exy.y += dEY[x]; }
       const cx<T> tprev = carry[x];

@@ -505,9 +505,14 @@ extern "C" int les_gpu_set_learned_guard(les_handle* h, double ratio) {
   return guarded(h, [&] { h->eng->set_learned_guard(ratio); });
 }
 
-extern "C" int les_gpu_learned_deardorff(les_handle* h, double* dissipation) {
+extern "C" int les_gpu_learned_reference(les_handle* h, double* dissipation) {
   if (!h || !dissipation) return LES_EINVAL;
-  return guarded(h, [&] { *dissipation = h->eng->learned_deardorff(); });
+  return guarded(h, [&] { *dissipation = h->eng->learned_reference(); });
+}
+
+extern "C" int les_gpu_learned_counts(les_handle* h, long long* stages, long long* used) {
+  if (!h) return LES_EINVAL;
+  return guarded(h, [&] { h->eng->learned_counts(stages, used); });
 }
 
 extern "C" int les_gpu_learn_filter(les_handle* h, int fxy, int fz, int with_model, double* out) {
@@ -518,11 +523,11 @@ extern "C" int les_gpu_learn_filter(les_handle* h, int fxy, int fz, int with_mod
   });
 }
 
-extern "C" int les_gpu_learned_features(les_handle* h, double re_tau, float* feat) {
-  if (!h || !feat || !(re_tau > 0)) return LES_EINVAL;
+extern "C" int les_gpu_learned_features(les_handle* h, float* feat) {
+  if (!h || !feat) return LES_EINVAL;
   if ((uintptr_t)feat % 16) { h->err = "les_gpu_learned_features: feat must be 16-byte aligned"; return LES_EINVAL; }
   return guarded(h, [&] {
-    h->eng->learned_features(re_tau, feat);
+    h->eng->learned_features(0.0, feat);
     LES_CUDA(cudaStreamSynchronize(h->eng->stream()));
   });
 }

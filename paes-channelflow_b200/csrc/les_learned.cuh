@@ -15,14 +15,23 @@
 //                 (the centred average of the w-level differences with
 //                  UZ(0) = UZ(1) and UZ(nnz) = UZ(nnz-1), as derivs1.f90 /
 //                  derivs2.f90 set the wall rows)
-//      and from them the normalised bf16 features (or raw f32 features);
-//   3. k_mlp_infer<MlpOutTau>: tau_ij on the tensor cores, and the per-CTA
-//      sums of the dissipation -tau_ij S_ij;
-//   4. k_deardorff_dissip + k_learned_flag: plane-and-level means (FP64,
-//      fixed order) of the network's dissipation -tau_ij S_ij and of the
-//      Deardorff model's 2 nu_t S_ij S_ij on the same state; flag = 1 when
-//      the network's is >= 0 and (guard > 0) within a factor guard of
-//      Deardorff's, else 0 (Deardorff fallback);
+//      and from them the normalised bf16 features (or raw f32 features):
+//      the closure is dimensionless, so that one network serves every grid
+//      and filter width:
+//        inputs  x_j = g_j / |G| (j = 0..8, g the nine gradients, |G| their
+//                Frobenius norm), min(z_w / Delta, kZwCap), z_w / h
+//                (z_w the distance to the nearest wall, h = zl / 2)
+//        outputs c_ij, tau_ij = (Delta |G|)^2 c_ij
+//      (an eddy viscosity is the special case c = -2 C^2 (|S|/|G|) S/|G|);
+//      Delta |G| rides along in bf16 columns 11 (high part) and 12 (the
+//      rounding remainder), which the network's padded first layer ignores;
+//   3. k_mlp_infer<MlpOutTau>: tau_ij on the tensor cores, and per CTA the
+//      sums of the network's dissipation -tau_ij S_ij and of the reference
+//      dissipation (0.1 Delta)^2 |S|^3 (the Smagorinsky estimate with the
+//      reference's imodel 4 constants, complen.f90:22-23);
+//   4. k_learned_flag: the means (FP64, fixed order); flag = 1 when the
+//      network's is >= 0 and (guard > 0) within a factor guard of the
+//      reference's, else 0 (Deardorff fallback);
 //   ... the padded-grid kernels (their interior momentum stresses are
 //      multiplied by 1 - flag) ...
 //   5. k_row_r2c + k_col_small: tau^ at every level;
@@ -83,14 +92,21 @@ template <int NX> struct LgxCfg {
   template <class T> static constexpr size_t smem() { return (size_t)(BUF + 10 * RB * (NX / 2)) * sizeof(cx<T>); }
 };
 
+// Cap of the wall-distance input z_w / Delta: farther from the wall than
+// kZwCap filter widths the closure sees one value.
+constexpr float kZwCap = 16.0f;
+
 // Gradients and features at the cell centres of RB rows (one level, RB
-// consecutive y) per block.  RAW: f32 [N][16] unnormalised features;
-// otherwise bf16 [N][16] normalised with P's in_shift / in_scale.
-// Feature order: (ux, vx, wx, uy, vy, wy, uz, vz, wz) * Delta, z+, Delta.
+// consecutive y) per block.  RAW: f32 [N][16] unnormalised features
+// x_0..x_10, Delta |G| in column 11, zeros in 12..15; otherwise bf16
+// [N][16]: x_0..x_10 normalised with P's in_shift / in_scale, Delta |G| as
+// bf16 high part (column 11) and remainder (column 12), zeros in 13..15.
+// x order: (ux, vx, wx, uy, vy, wy, uz, vz, wz) / |G|, min(z_w/Delta,
+// kZwCap), z_w / h.
 template <class T, int NX, bool RAW>
 __global__ void __launch_bounds__(LgxCfg<NX>::THREADS)
 k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* __restrict__ P, int NY, int NZ,
-          T kx0, T dzm, T delta, T dz, T zl, T zplus_per_len, const cx<T>* __restrict__ tw) {
+          T kx0, T dzm, T delta, T dz, T zl, T inv_h, const cx<T>* __restrict__ tw) {
   using L = LgxCfg<NX>;
   constexpr int KX = NX / 2, RB = L::RB;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -156,21 +172,33 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
     const T zc = ((T)z + (T)0.5) * dz;
     const T zw = zc < zl - zc ? zc : zl - zc;
     const size_t p = row * NX + x;
+    T g2 = (T)0;
+#pragma unroll
+    for (int j = 0; j < 9; j++) g2 += g[j] * g[j];
+    const T gm = sqrt(g2);
+    const T rg = gm > (T)0 ? (T)1 / gm : (T)0;
+    T xin[11];
+#pragma unroll
+    for (int j = 0; j < 9; j++) xin[j] = g[j] * rg;
+    const T zd = zw / delta;
+    xin[9] = zd < (T)kZwCap ? zd : (T)kZwCap;
+    xin[10] = zw * inv_h;
+    const float sc = (float)(gm * delta);  // Delta |G|
     if constexpr (RAW) {
       float4* o = reinterpret_cast<float4*>(feat) + 4 * p;
-      o[0] = make_float4((float)(g[0] * delta), (float)(g[1] * delta), (float)(g[2] * delta), (float)(g[3] * delta));
-      o[1] = make_float4((float)(g[4] * delta), (float)(g[5] * delta), (float)(g[6] * delta), (float)(g[7] * delta));
-      o[2] = make_float4((float)(g[8] * delta), (float)(zw * zplus_per_len), (float)delta, 0.f);
+      o[0] = make_float4((float)xin[0], (float)xin[1], (float)xin[2], (float)xin[3]);
+      o[1] = make_float4((float)xin[4], (float)xin[5], (float)xin[6], (float)xin[7]);
+      o[2] = make_float4((float)xin[8], (float)xin[9], (float)xin[10], sc);
       o[3] = make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
       float f[11];
 #pragma unroll
-      for (int jj = 0; jj < 9; jj++) f[jj] = (float)((g[jj] * delta - (T)P->in_shift[jj]) * (T)P->in_scale[jj]);
-      f[9] = (float)((zw * zplus_per_len - (T)P->in_shift[9]) * (T)P->in_scale[9]);
-      f[10] = (float)((delta - (T)P->in_shift[10]) * (T)P->in_scale[10]);
+      for (int jj = 0; jj < 11; jj++) f[jj] = (float)((xin[jj] - (T)P->in_shift[jj]) * (T)P->in_scale[jj]);
+      const __nv_bfloat16 shi = __float2bfloat16_rn(sc);
+      const float slo = sc - __bfloat162float(shi);
       uint4* o = reinterpret_cast<uint4*>(feat) + 2 * p;
       o[0] = make_uint4(pack_bf2(f[0], f[1]), pack_bf2(f[2], f[3]), pack_bf2(f[4], f[5]), pack_bf2(f[6], f[7]));
-      o[1] = make_uint4(pack_bf2(f[8], f[9]), pack_bf2(f[10], 0.f), 0u, 0u);
+      o[1] = make_uint4(pack_bf2(f[8], f[9]), pack_bf2(f[10], sc), pack_bf2(slo, 0.f), 0u);
     }
   }
 }
@@ -178,98 +206,65 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
 __device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
 
+// Delta |G| from the bf16 columns 11 (high part) and 12 (remainder).
+__device__ __forceinline__ float feat_scale(uint4 f1) { return bf_hi(f1.y) + bf_lo(f1.z); }
+
 // Network outputs -> tau planes [6][N] (tau11, tau22, tau33, tau12, tau13,
-// tau23), planes 6, 7: tau13 g_uz + tau23 g_vz and g_uz^2 + g_vz^2 (g = the
-// gradients times Delta, for the network's effective viscosity), and the
-// dissipation -tau_ij S_ij * Delta from the features.
+// tau23) = (Delta |G|)^2 (y * out_scale + out_shift); planes 6, 7:
+// tau13 g_uz + tau23 g_vz and g_uz^2 + g_vz^2 (g = the gradients times
+// Delta, for the network's effective viscosity); returns the network's
+// dissipation -tau_ij S_ij and the reference (0.1 Delta)^2 |S|^3, each
+// times Delta (k_learned_flag divides the sums by N Delta).
 template <class T> struct MlpOutTau {
   T* tau;  // [8][N]
   long long N;
-  __device__ double operator()(long long p, bool valid, const float (&y)[16], uint4 f0, uint4 f1,
-                               const MlpDev* P) const {
-    if (!valid) return 0.0;
+  __device__ double2 operator()(long long p, bool valid, const float (&y)[16], uint4 f0, uint4 f1,
+                                const MlpDev* P) const {
+    if (!valid) return make_double2(0.0, 0.0);
+    const float s = feat_scale(f1);
+    const float s2 = s * s;
     float t[6];
 #pragma unroll
     for (int i = 0; i < 6; i++) {
-      t[i] = y[i] * P->out_scale[i] + P->out_shift[i];
+      t[i] = s2 * (y[i] * P->out_scale[i] + P->out_shift[i]);
       tau[(size_t)i * N + p] = (T)t[i];
     }
     const float q[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
                         bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
     float g[9];
 #pragma unroll
-    for (int j = 0; j < 9; j++) g[j] = q[j] * P->in_rscale[j] + P->in_shift[j];  // d_i u_j * Delta
+    for (int j = 0; j < 9; j++) g[j] = (q[j] * P->in_rscale[j] + P->in_shift[j]) * s;  // d_i u_j * Delta
     tau[(size_t)6 * N + p] = (T)(t[4] * g[6] + t[5] * g[7]);
     tau[(size_t)7 * N + p] = (T)(g[6] * g[6] + g[7] * g[7]);
     const float s11 = g[0], s22 = g[4], s33 = g[8];
     const float s12 = 0.5f * (g[3] + g[1]), s13 = 0.5f * (g[6] + g[2]), s23 = 0.5f * (g[7] + g[5]);
-    return -((double)t[0] * s11 + (double)t[1] * s22 + (double)t[2] * s33 +
-             2.0 * ((double)t[3] * s12 + (double)t[4] * s13 + (double)t[5] * s23));
+    const double ss = 2.0 * ((double)s11 * s11 + (double)s22 * s22 + (double)s33 * s33 +
+                             2.0 * ((double)s12 * s12 + (double)s13 * s13 + (double)s23 * s23));  // (|S| Delta)^2
+    const double net = -((double)t[0] * s11 + (double)t[1] * s22 + (double)t[2] * s33 +
+                         2.0 * ((double)t[3] * s12 + (double)t[4] * s13 + (double)t[5] * s23));
+    return make_double2(net, 0.01 * ss * sqrt(ss));
   }
 };
 
-// Deardorff partial sums for the fallback test: per cell centre 2 nu_t
-// S_ij S_ij, with S from the staged bf16 features (the gradients times
-// Delta, as the network sees them), nu_t = min(c01 sqrt(e_c), xkmax) + nu
-// and e_c = (e(k-1) + e(k)) / 2, e(0) read as e(1) (e1 = e at level 1,
-// levels ps apart).  Each term is divided by Delta^2 and multiplied by
-// Delta, the scale of the network's sums (k_learned_flag divides both by
-// N Delta).  Grid (gridDim.x, NZ): blockIdx.y = level - 1, a grid-stride
-// over the level's ps points; part[level][blockIdx.x] = the block's sum.
-template <class T>
-__global__ void __launch_bounds__(256) k_deardorff_dissip(const uint4* __restrict__ feat, const T* __restrict__ e1,
-                                                          const MlpDev* __restrict__ P, int ps, T c01, T xkmax,
-                                                          T nu, T inv_delta, double* __restrict__ part) {
-  __shared__ double red[8];
-  const int k = blockIdx.y;
-  const T* ek = e1 + (size_t)k * ps;
-  const T* em = e1 + (size_t)(k > 0 ? k - 1 : 0) * ps;  // e(0) read as e(1)
-  const uint4* fk = feat + (size_t)2 * k * ps;
-  float rs[9], sh[9];
-#pragma unroll
-  for (int j = 0; j < 9; j++) { rs[j] = P->in_rscale[j]; sh[j] = P->in_shift[j]; }
-  double acc = 0.0;
-  for (int i = blockIdx.x * 256 + threadIdx.x; i < ps; i += gridDim.x * 256) {
-    const uint4 f0 = fk[2 * i], f1 = fk[2 * i + 1];
-    const float q[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
-                        bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
-    float g[9];
-#pragma unroll
-    for (int j = 0; j < 9; j++) g[j] = q[j] * rs[j] + sh[j];  // d_i u_j * Delta
-    const T ec = (T)0.5 * (em[i] + ek[i]);
-    const T nut = tmin(c01 * sqrt(tmax(ec, (T)0)), xkmax) + nu;
-    const float s11 = g[0], s22 = g[4], s33 = g[8];
-    const float s12 = 0.5f * (g[3] + g[1]), s13 = 0.5f * (g[6] + g[2]), s23 = 0.5f * (g[7] + g[5]);
-    const double ss = (double)s11 * s11 + (double)s22 * s22 + (double)s33 * s33 +
-                      2.0 * ((double)s12 * s12 + (double)s13 * s13 + (double)s23 * s23);
-    acc += 2.0 * (double)nut * ss * (double)inv_delta;
-  }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < 8; w++) s += red[w];
-    part[(size_t)k * gridDim.x + blockIdx.x] = s;
-  }
-}
-
-// Mean dissipations (per-CTA sums in CTA order) -> flag and status
-// [network mean, flag, Deardorff mean].  guard <= 0: the sign test only.
-static __global__ void k_learned_flag(const double* __restrict__ part, int nparts, const double* __restrict__ partd,
-                                      int npartd, double inv_n_delta, double guard, int* __restrict__ flag,
-                                      double* __restrict__ status) {
+// Mean dissipations (per-CTA pairs of sums in CTA order: the network's,
+// the reference's) -> flag, status [network mean, flag, reference mean] and
+// the stage counters [stages, stages that used the network].  guard <= 0:
+// the sign test only.
+static __global__ void k_learned_flag(const double* __restrict__ part, int nparts, double inv_n_delta, double guard,
+                                      int* __restrict__ flag, double* __restrict__ status,
+                                      unsigned long long* __restrict__ counts) {
   if (threadIdx.x != 0) return;
-  double s = 0.0, sd = 0.0;
-  for (int i = 0; i < nparts; i++) s += part[i];
-  for (int i = 0; i < npartd; i++) sd += partd[i];
-  const double mean = s * inv_n_delta, meand = sd * inv_n_delta;
+  double s = 0.0, sr = 0.0;
+  for (int i = 0; i < nparts; i++) { s += part[2 * i]; sr += part[2 * i + 1]; }
+  const double mean = s * inv_n_delta, meanr = sr * inv_n_delta;
   int use = (mean >= 0.0) ? 1 : 0;  // NaN -> fallback
-  if (guard > 0.0 && !(meand > 0.0 && mean <= guard * meand && guard * mean >= meand)) use = 0;
+  if (guard > 0.0 && !(meanr > 0.0 && mean <= guard * meanr && guard * mean >= meanr)) use = 0;
   flag[0] = use;
   status[0] = mean;
   status[1] = (double)use;
-  status[2] = meand;
+  status[2] = meanr;
+  counts[0] += 1ull;
+  counts[1] += (unsigned long long)use;
 }
 
 // Per-level partial sums of tau planes 6 and 7 (MlpOutTau): grid (NZ,
@@ -374,17 +369,19 @@ namespace les {
 
 // ---------------------------------------------------------------------------
 // Training data of the learned closure: explicit filtering of a fine run.
-// z: box average over the fz fine cells of each coarse cell (fz = 1 or 2);
+// z: box average over the fz fine cells of each coarse cell (fz = 1 or even);
 // x, y: the box filter of width Delta_c (the coarse cell) as the spectral
 // transfer sin(k Delta_c / 2) / (k Delta_c / 2), then truncation to the
 // coarse modes (|kx| < nxc/2, |ky| < nyc/2; the truncation of redim.f90:
 // 277-318 without its Nyquist rows).  Filtered quantities at the coarse
 // cell centres: u, v, wc, uu, vv, wc wc, u v, u wc, v wc (wc = w averaged to
-// the fine centres), and w at the coarse w-levels (fz = 2: weights 1/4,
-// 1/2, 1/4 of the fine w-levels 2K-1, 2K, 2K+1).
+// the fine centres), and w at the coarse w-levels: the box of width fz fine
+// cells centred on the coarse face K (fine face fz K) by the trapezoid rule,
+// weights 1/(2 fz) on the fine faces fz K -/+ fz/2 and 1/fz between (fz = 2:
+// 1/4, 1/2, 1/4 of the fine w-levels 2K-1, 2K, 2K+1).
 // ---------------------------------------------------------------------------
-// With F (the fine run's raw features at the cell centres, f32 [NZ*ps][16],
-// whose first nine columns are the gradients times dsl)
+// With F (the fine run's raw features at the cell centres, f32 [NZ*ps][16]:
+// columns 0..8 the gradients over |G|, column 11 dsl |G|)
 // and E (its TKE at the w-levels, plane k = level k), the fine run's own
 // Deardorff stress -2 nu_t S_ij, nu_t = 0.1 dsl sqrt(max(e_c, emin)) with e_c
 // the average of the two faces of the cell (faces 0 and nnz take the values
@@ -413,8 +410,9 @@ __global__ void k_filt_z(const T* __restrict__ U, const T* __restrict__ V, const
     if (F) {
       const size_t o = (size_t)(k - 1) * ps + p;
       T g[9];
+      const T gs = (T)F[o * 16 + 11] / dsl;  // |G|
 #pragma unroll
-      for (int i = 0; i < 9; i++) g[i] = (T)F[o * 16 + i] / dsl;  // ux, vx, wx, uy, vy, wy, uz, vz, wz
+      for (int i = 0; i < 9; i++) g[i] = (T)F[o * 16 + i] * gs;  // ux, vx, wx, uy, vy, wy, uz, vz, wz
       T ec = (T)0.5 * (ef(k) + ef(k - 1));
       ec = ec > emin ? ec : emin;
       const T nu2 = (T)0.2 * dsl * sqrt(ec);
@@ -430,7 +428,13 @@ __global__ void k_filt_z(const T* __restrict__ U, const T* __restrict__ V, const
   const size_t plane = (size_t)NZc * ps;
 #pragma unroll
   for (int i = 0; i < 9; i++) S[i * plane + (size_t)(K - 1) * ps + p] = q[i] * inv;
-  const T wst = (fz == 2) ? (T)0.25 * w(2 * K - 1) + (T)0.5 * w(2 * K) + (T)0.25 * w(2 * K + 1) : w(K);
+  T wst = w(K);
+  if (fz > 1) {
+    const int c = fz * K, hf = fz / 2;
+    wst = (T)0.5 * (w(c - hf) + w(c + hf));
+    for (int j = c - hf + 1; j < c + hf; j++) wst += w(j);
+    wst *= inv;
+  }
   S[9 * plane + (size_t)(K - 1) * ps + p] = wst;
 }
 

@@ -134,14 +134,15 @@ def lib():
         "les_gpu_set_mlp": (I, [H, VP, D]),
         "les_gpu_learned_status": (I, [H, ctypes.POINTER(I), ctypes.POINTER(D)]),
         "les_gpu_set_learned_guard": (I, [H, D]),
-        "les_gpu_learned_deardorff": (I, [H, ctypes.POINTER(D)]),
+        "les_gpu_learned_reference": (I, [H, ctypes.POINTER(D)]),
+        "les_gpu_learned_counts": (I, [H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "les_gpu_learn_filter": (I, [H, I, I, I, VP]),
         "les_gpu_write_field": (I, [H, ctypes.c_char_p, D, I, I]),
         "les_gpu_field_wait": (I, [H]),
         "les_gpu_read_field": (I, [H, ctypes.c_char_p, I, ctypes.POINTER(D)]),
         "les_gpu_regrid": (I, [H, H]),
         "les_gpu_field_header": (I, [ctypes.c_char_p, I, ctypes.POINTER(I), ctypes.POINTER(D)]),
-        "les_gpu_learned_features": (I, [H, D, VP]),
+        "les_gpu_learned_features": (I, [H, VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -295,15 +296,22 @@ class LesGpu:
         return used.value, d.value
 
     def set_learned_guard(self, ratio):
-        """Factor of the fallback test against the Deardorff dissipation
-        (default 4; <= 0 keeps only the sign test)."""
+        """Factor of the fallback test against the reference (Smagorinsky)
+        dissipation (default 4; <= 0 keeps only the sign test)."""
         self._check(lib().les_gpu_set_learned_guard(self.h, float(ratio)))
 
-    def learned_deardorff(self):
-        """Deardorff mean dissipation of the last learned stage (synchronising)."""
+    def learned_reference(self):
+        """Reference (Smagorinsky) mean dissipation of the last learned
+        stage (synchronising)."""
         d = ctypes.c_double()
-        self._check(lib().les_gpu_learned_deardorff(self.h, ctypes.byref(d)))
+        self._check(lib().les_gpu_learned_reference(self.h, ctypes.byref(d)))
         return d.value
+
+    def learned_counts(self):
+        """(stages evaluated, stages that used the network) since set_mlp."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(lib().les_gpu_learned_counts(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def learn_filter(self, fxy, fz, with_model=True):
         """Filtered coarse fields of the current state: float64 CUDA tensor
@@ -317,12 +325,13 @@ class LesGpu:
         self._check(lib().les_gpu_learn_filter(self.h, fxy, fz, int(with_model), out.data_ptr()))
         return out
 
-    def learned_features(self, re_tau):
-        """Raw network inputs at every cell centre: float32 CUDA tensor (N, 16)."""
+    def learned_features(self):
+        """Raw network inputs at every cell centre: float32 CUDA tensor
+        (N, 16), columns 0..10 the inputs, column 11 Delta |G|."""
         import torch
         c = self.cfg
         out = torch.empty((c.nnx * c.nny * c.nnz, 16), dtype=torch.float32, device="cuda:%d" % c.device)
-        self._check(lib().les_gpu_learned_features(self.h, re_tau, out.data_ptr()))
+        self._check(lib().les_gpu_learned_features(self.h, out.data_ptr()))
         return out
 
     def write_field(self, path, time=0.0, real_bytes=8, background=False):

@@ -1,38 +1,44 @@
 """Training of the learned sub-grid closure on one GPU.
 
-    python paes-channelflow_b200/train_closure.py [--fine 384 384 192] [--factor 4 2]
-        [--re-tau 395] [--snapshots 200] [--spinup 14000] [--every 40] [--epochs 20]
-        [--aposteriori 4000] [--out paes-channelflow_b200/weights/sgs_c4]
+    python paes-channelflow_b200/train_closure.py [--fine 384 384 192] [--factors 2 4]
+        [--re-tau 395] [--snapshots 100] [--spinup 14000] [--every 60] [--epochs 12]
+        [--out paes-channelflow_b200/weights/sgs_c4]
+
+The closure is dimensionless (les_mlp.h): inputs g/|G| (the nine resolved
+velocity gradients over their Frobenius norm), min(z_w/Delta, 16) and z_w/h,
+outputs c with tau_ij = (Delta |G|)^2 c_ij.  Trained on several filter
+widths Delta of the same fine run, it learns the stress per (Delta |G|)^2 as
+a function of the local flow geometry and the wall distance in filter
+widths, which is what carries it from the training grids to others.
 
 1. A fine run of this solver (Deardorff closure) from the log-law mean
    profile of the wall model plus random perturbations (small-scale noise
    and large structures, which make the flow transition within a few eddy
    turnovers); the spin-up runs in the mixed form, then the state moves to
    an FP64 handle for the data.
-2. After the spin-up, every `every` steps: les_gpu_learn_filter onto the
-   coarse grid (box filter: `fxy` fine cells in x, y and `fz` in z) gives
-   the filtered u, v, w and tau_ij = filt(u_i u_j) - filt(u_i) filt(u_j)
-   plus (by default) the filtered Deardorff stress of the fine run itself,
-   i.e. the total sub-filter stress the coarse grid misses (without it the
-   targets lack the momentum flux the fine run's model carries near the
-   walls, and coarse runs with the network lose their near-wall velocity);
-   the filtered fields are loaded into a coarse handle whose
-   les_gpu_learned_features computes the network inputs with the same
-   kernels the learned stage uses.
-3. Normalisation (mean / standard deviation per input and output) from the
-   training snapshots; the last `holdout` fraction of snapshots is held out.
+2. After the spin-up, every `every` steps and for every filter factor f:
+   les_gpu_learn_filter onto the grid (nx/f, ny/f, nz/f) (box filter of f
+   fine cells in x, y and z, so the coarse cells keep the fine cells' aspect
+   ratio) gives the filtered u, v, w and tau_ij = filt(u_i u_j) -
+   filt(u_i) filt(u_j) plus (by default) the filtered Deardorff stress of
+   the fine run itself, i.e. the total sub-filter stress the coarse grid
+   misses; the filtered fields are loaded into a coarse handle whose
+   les_gpu_learned_features computes the network inputs (and Delta |G|)
+   with the same kernels the learned stage uses.
+3. Targets: the deviatoric stress over (Delta |G|)^2, clipped to the
+   training set's 99.9th percentile of |c| per component (points where |G|
+   is tiny carry stresses the local gradients cannot explain); normalisation
+   (mean / standard deviation per input and output) from the training
+   snapshots; the last `holdout` fraction of snapshots is held out.
 4. Adam (lr 1e-3, batch 65536, f32 master weights) on the tensor-core
-   kernels (les_mlp_adam_step), shuffled batches, `epochs` passes.
-5. A-priori evaluation on the held-out snapshots: per-component
-   correlation coefficient and normalised MSE of the deviatoric stresses,
-   for the network and for the Deardorff eddy viscosity
-   tau_ij^dev = -2 (0.1 Delta sqrt(e)) S_ij with the filtered e = tau_kk / 2.
-6. A-posteriori (optional): coarse runs from the first filtered snapshot
-   with the Deardorff closure and with the network; mean U(z) against the
-   filtered fine run's mean profile.
-7. Writes <out>.npz (params, norm, re_tau, grids), <out>.json (report) and
-   <out>_eval.npz (the first filtered snapshot and the filtered fine run's
-   mean profile; --evaluate repeats step 6 from it).
+   kernels (les_mlp_adam_step), shuffled batches over all filter widths.
+5. A-priori evaluation per filter width on the held-out snapshots: per
+   component correlation and normalised MSE of the deviatoric stresses for
+   the network, for the Deardorff eddy viscosity -2 (0.1 Delta sqrt(e)) S
+   with the filtered e = tau_kk / 2, and for Smagorinsky -2 (0.1 Delta)^2
+   |S| S; mean dissipations of the network, the filtered truth and the
+   Smagorinsky estimate the runtime fallback test compares with.
+6. Writes <out>.npz (params, norm, grids) and <out>.json (report).
 """
 import argparse
 import importlib.util
@@ -44,6 +50,7 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+COMPONENTS = ("tau11", "tau22", "tau33", "tau12", "tau13", "tau23")
 
 
 def _host():
@@ -87,15 +94,18 @@ def loglaw_field(cfg, amp, seed, large=0.0, utau=float(np.sqrt(0.016)), kappa=0.
     return u, v, w, e
 
 
-def collect(fine=(384, 384, 192), factor=(4, 2), re_tau=395.0, snapshots=200, spinup=14000, every=40, amp=1.0,
+def delta_of(grid, xl=2 * np.pi, yl=np.pi, zl=2.0):
+    nx, ny, nz = grid
+    return (xl / nx * yl / ny * zl / nz) ** (1.0 / 3.0)
+
+
+def collect(fine=(384, 384, 192), factors=(2, 4), re_tau=395.0, snapshots=100, spinup=14000, every=60, amp=1.0,
             large=0.3, seed=12345, cfl=0.5, spinup_precision=4, with_model=True, log=print):
-    """Run the fine case and return (features f32 (S, Nc, 16), targets f64
-    (S, Nc, 6), info, first filtered (u, v, w)) with the sample arrays as
-    CUDA tensors."""
+    """Run the fine case; returns ({factor: (features f32 (S, Nc, 16), stresses
+    f32 (S, Nc, 6))} as CUDA tensors, info)."""
     import torch
     P = _host()
     nx, ny, nz = fine
-    fxy, fz = factor
     t0 = time.time()
     cfg = P.channel_config(nx, ny, nz, dt=1e-3, re_tau=re_tau, precision=spinup_precision)
     g = P.LesGpu(cfg)
@@ -128,63 +138,110 @@ def collect(fine=(384, 384, 192), factor=(4, 2), re_tau=395.0, snapshots=200, sp
         g = P.LesGpu(cfg)
         g.upload(f["u"], f["v"], f["w"], f["e"], f["p"])
         del f
-    ccfg = P.channel_config(nx // fxy, ny // fxy, nz // fz, dt=dt, re_tau=re_tau, precision=8)
-    ccfg.z0 = cfg.z0
-    c = P.LesGpu(ccfg)
-    nc = (nx // fxy) * (ny // fxy) * (nz // fz)
-    feats = torch.empty((snapshots, nc, 16), dtype=torch.float32, device="cuda")
-    targs = torch.empty((snapshots, nc, 6), dtype=torch.float64, device="cuda")
-    fine_means = []
-    first = None
+    coarse, data = {}, {}
+    for fac in factors:
+        ccfg = P.channel_config(nx // fac, ny // fac, nz // fac, dt=dt, re_tau=re_tau, precision=8)
+        ccfg.z0 = cfg.z0
+        nc = (nx // fac) * (ny // fac) * (nz // fac)
+        coarse[fac] = P.LesGpu(ccfg)
+        data[fac] = (torch.empty((snapshots, nc, 16), dtype=torch.float32, device="cuda"),
+                     torch.empty((snapshots, nc, 6), dtype=torch.float32, device="cuda"))
     for s in range(snapshots):
         if s > 0:
             for _ in range(every):
                 g.step(it=state["it"], mnout=False, dt=dt)
                 state["it"] += 1
-        out = g.learn_filter(fxy, fz, with_model=with_model)
-        uvw = out[:3].cpu().numpy()
-        if first is None:
-            first = uvw.copy()
-        c.upload(uvw[0], uvw[1], uvw[2], np.full_like(uvw[0], 1e-4), None)
-        feats[s] = c.learned_features(re_tau)
-        targs[s] = out[3:].reshape(6, nc).t()
-        fine_means.append(uvw[0].mean(axis=(1, 2)))
+        for fac in factors:
+            out = g.learn_filter(fac, fac, with_model=with_model)
+            uvw = out[:3].cpu().numpy()
+            c = coarse[fac]
+            c.upload(uvw[0], uvw[1], uvw[2], np.full_like(uvw[0], 1e-4), None)
+            data[fac][0][s] = c.learned_features()
+            data[fac][1][s] = out[3:].reshape(6, -1).t().float()
         if s == 0 or (s + 1) % max(1, snapshots // 10) == 0:
             monitor(g, "snapshot %d/%d" % (s + 1, snapshots))
     g.sync()
-    info = dict(fine=list(fine), factor=list(factor), re_tau=re_tau, snapshots=snapshots, spinup=spinup,
+    info = dict(fine=list(fine), factors=list(factors), re_tau=re_tau, snapshots=snapshots, spinup=spinup,
                 spinup_precision=spinup_precision, every=every, amp=amp, large=large, seed=seed, dt=dt,
                 targets="filtered total sub-filter stress" if with_model else "filtered minus resolved products",
-                steps=state["it"], coarse=[nx // fxy, ny // fxy, nz // fz], history=hist,
-                collect_seconds=time.time() - t0, filtered_mean_u=np.mean(fine_means, axis=0).tolist(), z0=cfg.z0)
+                steps=state["it"], coarse={str(f): [nx // f, ny // f, nz // f] for f in factors}, history=hist,
+                collect_seconds=time.time() - t0, z0=cfg.z0)
     g.close()
-    c.close()
-    return feats, targs, info, first
+    for c in coarse.values():
+        c.close()
+    return data, info
 
 
-def normalisation(feats, targs):
-    """in_shift, in_scale per input, out_scale, out_shift per output (34
-    floats); a constant input (the filter width on one grid) gets scale 0."""
+def deviatoric(t):
+    """(N, 6) stresses -> deviatoric (trace removed from the diagonal)."""
+    d = t.clone()
+    tr = (t[:, 0] + t[:, 1] + t[:, 2]) / 3.0
+    for i in range(3):
+        d[:, i] = t[:, i] - tr
+    return d
+
+
+def targets(feats, tau, clip=None):
+    """c = tau_dev / (Delta |G|)^2 of (N, 16) raw features and (N, 6)
+    stresses (float64); clip: per-component bound on |c| (None: none)."""
     import torch
-    f = feats.reshape(-1, 16)[:, :11].double()
-    t = targs.reshape(-1, 6)
-    fm, fs = f.mean(0), f.std(0)
-    tm, ts = t.mean(0), t.std(0)
+    s2 = feats[:, 11].double() ** 2
+    c = deviatoric(tau.double()) / torch.where(s2 > 0, s2, torch.ones_like(s2))[:, None]
+    c[s2 <= 0] = 0.0
+    if clip is not None:
+        c = torch.maximum(torch.minimum(c, clip[None, :]), -clip[None, :])
+    return c
+
+
+def clip_bounds(data, train_snaps, q=0.999, sample=4_000_000):
+    """99.9th percentile of |c| per component over a sample of the training
+    points of every filter width."""
+    import torch
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0)
+    cs = []
+    for fac, (f, t) in data.items():
+        ff = f[:train_snaps].reshape(-1, 16)
+        tt = t[:train_snaps].reshape(-1, 6)
+        idx = torch.randint(0, ff.shape[0], (min(sample, ff.shape[0]),), device="cuda", generator=gen)
+        cs.append(targets(ff[idx], tt[idx]).abs())
+    return torch.quantile(torch.cat(cs), q, dim=0)
+
+
+def normalisation(data, train_snaps, clip):
+    """in_shift, in_scale per input, out_scale, out_shift per output (34
+    floats) from the training snapshots of every filter width."""
+    import torch
+    n = 0
+    s1 = torch.zeros(11, dtype=torch.float64, device="cuda")
+    s2 = torch.zeros(11, dtype=torch.float64, device="cuda")
+    t1 = torch.zeros(6, dtype=torch.float64, device="cuda")
+    t2 = torch.zeros(6, dtype=torch.float64, device="cuda")
+    for fac, (f, t) in data.items():
+        for s in range(train_snaps):
+            x = f[s][:, :11].double()
+            c = targets(f[s], t[s], clip)
+            s1 += x.sum(0); s2 += (x * x).sum(0)
+            t1 += c.sum(0); t2 += (c * c).sum(0)
+            n += x.shape[0]
+    fm, tm = s1 / n, t1 / n
+    fs = torch.sqrt(torch.clamp(s2 / n - fm * fm, min=0.0))
+    ts = torch.sqrt(torch.clamp(t2 / n - tm * tm, min=1e-30))
     in_scale = torch.where(fs > 1e-6 * (fm.abs() + 1e-30), 1.0 / fs, torch.zeros_like(fs))
-    norm = np.concatenate([fm.cpu().numpy(), in_scale.cpu().numpy(), ts.cpu().numpy(), tm.cpu().numpy()])
+    norm = torch.cat([fm, in_scale, ts, tm]).cpu().numpy()
     return norm.astype(np.float32)
 
 
-def to_training(feats, targs, norm):
-    """bf16 normalised features (N, 16) and f32 normalised targets (N, 8)."""
+def to_training(feats, tau, norm, clip):
+    """bf16 normalised features (N, 16) and f32 normalised targets (N, 8)
+    of (N, 16) raw features and (N, 6) stresses."""
     import torch
     n = torch.from_numpy(norm.astype(np.float64)).to(feats.device)
-    f = feats.reshape(-1, 16).double()
-    x = torch.zeros_like(f)
-    x[:, :11] = (f[:, :11] - n[:11]) * n[11:22]
-    t = targs.reshape(-1, 6)
-    y = torch.zeros((t.shape[0], 8), dtype=torch.float32, device=t.device)
-    y[:, :6] = ((t - n[28:34]) / n[22:28]).float()
+    x = torch.zeros((feats.shape[0], 16), dtype=torch.float64, device=feats.device)
+    x[:, :11] = (feats[:, :11].double() - n[:11]) * n[11:22]
+    c = targets(feats, tau, clip)
+    y = torch.zeros((feats.shape[0], 8), dtype=torch.float32, device=feats.device)
+    y[:, :6] = ((c - n[28:34]) / n[22:28]).float()
     return x.to(torch.bfloat16).contiguous(), y.contiguous()
 
 
@@ -203,7 +260,7 @@ def init_params(seed=0):
     return p
 
 
-def train(mlp, x, y, epochs=20, batch=65536, lr=1e-3, seed=0, log=print):
+def train(mlp, x, y, epochs=12, batch=65536, lr=1e-3, seed=0, log=print):
     import torch
     gen = torch.Generator(device=x.device)
     gen.manual_seed(seed)
@@ -226,188 +283,116 @@ def train(mlp, x, y, epochs=20, batch=65536, lr=1e-3, seed=0, log=print):
     return hist, step, time.time() - t0
 
 
-def deviatoric(t):
-    """(N, 6) stresses -> deviatoric (trace removed from the diagonal)."""
-    d = t.clone()
-    tr = (t[:, 0] + t[:, 1] + t[:, 2]) / 3.0
-    for i in range(3):
-        d[:, i] = t[:, i] - tr
-    return d
-
-
-def apriori(mlp, feats, targs, norm, delta):
-    """Correlation coefficient and normalised MSE per deviatoric component,
-    network vs Deardorff's eddy viscosity, on (S, Nc, ...) held-out data."""
+def apriori(mlp, feats, tau, norm, clip, delta):
+    """Per deviatoric component: correlation and normalised MSE of the
+    network's stresses, of Deardorff's eddy viscosity (filtered e) and of
+    Smagorinsky's, against the filtered truth; mean dissipations.  feats
+    (N, 16) raw features, tau (N, 6) stresses of held-out snapshots."""
     import torch
-    x, _ = to_training(feats, targs, norm)
-    yhat = mlp.forward(x)[:, :6].double()
-    n = torch.from_numpy(norm.astype(np.float64)).to(yhat.device)
-    tau_net = yhat * n[22:28] + n[28:34]
-    tau = targs.reshape(-1, 6)
-    f = feats.reshape(-1, 16).double()
-    g = f[:, :9] / delta  # (ux, vx, wx, uy, vy, wy, uz, vz, wz)
+    x, _ = to_training(feats, tau, norm, clip)
+    y = mlp.forward(x)[:, :6].double()
+    n = torch.from_numpy(norm.astype(np.float64)).to(y.device)
+    s = feats[:, 11].double()
+    tau_net = (y * n[22:28] + n[28:34]) * (s * s)[:, None]
+    t = tau.double()
+    g = feats[:, :9].double() * (s / delta)[:, None]  # (ux, vx, wx, uy, vy, wy, uz, vz, wz)
     S = torch.stack([g[:, 0], g[:, 4], g[:, 8], 0.5 * (g[:, 3] + g[:, 1]), 0.5 * (g[:, 6] + g[:, 2]),
                      0.5 * (g[:, 7] + g[:, 5])], dim=1)
-    e = torch.clamp(0.5 * (tau[:, 0] + tau[:, 1] + tau[:, 2]), min=0.0)
-    nut = 0.1 * delta * torch.sqrt(e)
-    tau_dd = -2.0 * nut[:, None] * S
-    td, nd, dd = deviatoric(tau), deviatoric(tau_net), deviatoric(tau_dd)
-    names = ["tau11", "tau22", "tau33", "tau12", "tau13", "tau23"]
+    w = torch.tensor([1.0, 1.0, 1.0, 2.0, 2.0, 2.0], dtype=torch.float64, device=S.device)
+    smag = torch.sqrt(2.0 * (S * S * w).sum(1))
+    e = torch.clamp(0.5 * (t[:, 0] + t[:, 1] + t[:, 2]), min=0.0)
+    tau_dd = -2.0 * (0.1 * delta * torch.sqrt(e))[:, None] * S
+    tau_sm = -2.0 * ((0.1 * delta) ** 2 * smag)[:, None] * S
+    td = deviatoric(t)
     rep = {}
-    for i, nm in enumerate(names):
+    for i, nm in enumerate(COMPONENTS):
         a = td[:, i]
         var = float(((a - a.mean()) ** 2).mean())
         r = {}
-        for lab, p in (("network", nd[:, i]), ("deardorff", dd[:, i])):
+        for lab, p in (("network", deviatoric(tau_net)[:, i]), ("deardorff", deviatoric(tau_dd)[:, i]),
+                       ("smagorinsky", deviatoric(tau_sm)[:, i])):
             rho = float(torch.corrcoef(torch.stack([a, p]))[0, 1])
             mse = float(((p - a) ** 2).mean()) / max(var, 1e-300)
             r[lab] = dict(rho=rho, nmse=mse)
         rep[nm] = r
-    w = torch.tensor([1.0, 1.0, 1.0, 2.0, 2.0, 2.0], dtype=torch.float64, device=S.device)
-    rep["dissipation"] = dict(network=float((-(tau_net * S * w).sum(1)).mean()),
-                              filtered=float((-(tau * S * w).sum(1)).mean()))
+    dis = lambda tt: float((-(tt * S * w).sum(1)).mean())
+    rep["dissipation"] = dict(network=dis(tau_net), filtered=dis(t), deardorff=dis(tau_dd),
+                              smagorinsky_reference=float((0.01 * delta ** 2 * smag ** 3).mean()))
+    rep["dissipation"]["network_over_reference"] = rep["dissipation"]["network"] / rep["dissipation"][
+        "smagorinsky_reference"]
     return rep
-
-
-def aposteriori(first, info, params, norm, nsteps, log=print, guard=0.0):
-    """Coarse runs from the first filtered snapshot with the Deardorff
-    closure and with the trained network; time-averaged mean U(z) over the
-    second half against the filtered fine run's mean profile.  guard: the
-    factor of the fallback test against the Deardorff dissipation for the
-    learned run (0: the sign test only, so the network itself is judged)."""
-    P = _host()
-    nxc, nyc, nzc = info["coarse"]
-    re_tau = info["re_tau"]
-    ref = np.array(info["filtered_mean_u"])
-    ub = float(ref.mean())
-    out = {}
-    for name, imodel in (("deardorff", 3), ("learned", 5)):
-        cfg = P.channel_config(nxc, nyc, nzc, dt=1e-3, re_tau=re_tau, imodel=imodel, precision=8)
-        cfg.z0 = info["z0"]
-        g = P.LesGpu(cfg)
-        g.upload(first[0], first[1], first[2], np.full_like(first[0], 1e-4), None)
-        m = None
-        if imodel == 5:
-            m = P.Mlp(params, norm)
-            g.set_mlp(m, re_tau)
-            g.set_learned_guard(guard)
-        dt = g.cfl_dt(0.5)
-        prof, used, nstat = [], 0, 0
-        t0 = time.time()
-        for it in range(nsteps):
-            g.step(it=it, mnout=False, dt=dt)
-            if it >= nsteps // 2 and it % 10 == 0:
-                mb, _ = g.stats()
-                prof.append(mb[3].copy())
-                if m is not None:
-                    used += g.learned_status()[0]
-                nstat += 1
-        g.sync()
-        U = np.mean(prof, axis=0)
-        err = np.abs(U - ref).max() / ub
-        out[name] = dict(mean_u=U.tolist(), max_err_vs_filtered_over_ub=float(err),
-                         used_fraction=(used / nstat if m is not None else None), seconds=time.time() - t0,
-                         steps=nsteps, dt=dt)
-        log("a posteriori %s: max |U - U_filtered| / U_b = %.4f" % (name, err))
-        g.close()
-        if m is not None:
-            m.close()
-    out["filtered_mean_u"] = ref.tolist()
-    return out
 
 
 def run(args, log=print):
     import torch
     P = _host()
     t_all = time.time()
-    feats, targs, info, first = collect(tuple(args.fine), tuple(args.factor), args.re_tau, args.snapshots,
-                                        args.spinup, args.every, args.amp, args.large, args.seed,
-                                        spinup_precision=args.spinup_precision,
-                                        with_model=not getattr(args, "resolved_only", False), log=log)
-    S = feats.shape[0]
+    data, info = collect(tuple(args.fine), tuple(args.factors), args.re_tau, args.snapshots, args.spinup,
+                         args.every, args.amp, args.large, args.seed, spinup_precision=args.spinup_precision,
+                         with_model=not getattr(args, "resolved_only", False), log=log)
+    S = args.snapshots
     nho = max(1, int(round(S * args.holdout)))
-    ftr, ttr = feats[:S - nho], targs[:S - nho]
-    fho, tho = feats[S - nho:], targs[S - nho:]
-    norm = normalisation(ftr, ttr)
-    x, y = to_training(ftr, ttr, norm)
-    log("training samples %d, held-out snapshots %d" % (x.shape[0], nho))
+    ntr = S - nho
+    clip = clip_bounds(data, ntr)
+    norm = normalisation(data, ntr, clip)
+    xs, ys = [], []
+    for fac, (f, t) in data.items():
+        x, y = to_training(f[:ntr].reshape(-1, 16), t[:ntr].reshape(-1, 6), norm, clip)
+        xs.append(x)
+        ys.append(y)
+    x, y = torch.cat(xs), torch.cat(ys)
+    del xs, ys
+    log("training samples %d, held-out snapshots %d per filter width" % (x.shape[0], nho))
     mlp = P.Mlp(init_params(args.seed), norm)
     hist, steps, secs = train(mlp, x, y, args.epochs, args.batch, args.lr, seed=args.seed, log=log)
+    nsamples = int(x.shape[0])
     del x, y
     torch.cuda.empty_cache()
-    nxc, nyc, nzc = info["coarse"]
-    xl, yl, zl = 2 * np.pi, np.pi, 2.0
-    delta = (xl / nxc * yl / nyc * zl / nzc) ** (1.0 / 3.0)
-    rep_ho = apriori(mlp, fho, tho, norm, delta)
+    rep_ho = {}
+    for fac, (f, t) in data.items():
+        grid = info["coarse"][str(fac)]
+        rep_ho[str(fac)] = apriori(mlp, f[ntr:].reshape(-1, 16), t[ntr:].reshape(-1, 6), norm, clip,
+                                   delta_of(grid))
+        rep_ho[str(fac)]["grid"] = grid
+        rep_ho[str(fac)]["delta"] = delta_of(grid)
     params, _ = mlp.get_params()
     mlp.close()
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
-    # what the a-posteriori runs need, for evaluating later closures without a new fine run
-    ev = dict(coarse=info["coarse"], re_tau=info["re_tau"], z0=info["z0"], filtered_mean_u=info["filtered_mean_u"])
-    np.savez(args.out + "_eval.npz", first=first, meta=json.dumps(ev))
-    apost = None
-    if args.aposteriori:
-        apost = aposteriori(first, info, params, norm, args.aposteriori, log, getattr(args, "guard", 0.0))
     np.savez(args.out + ".npz", params=params, norm=norm, re_tau=np.float64(args.re_tau),
-             coarse=np.array(info["coarse"]), fine=np.array(info["fine"]), factor=np.array(info["factor"]))
-    report = dict(data=info, training=dict(steps=steps, seconds=secs, batch=args.batch, lr=args.lr,
-                                           epochs=args.epochs, samples=int(ftr.shape[0] * ftr.shape[1]),
-                                           samples_per_s=steps * args.batch / max(secs, 1e-9),
-                                           loss=hist[::max(1, len(hist) // 50)] + hist[-1:]),
-                  apriori_heldout=rep_ho, aposteriori=apost, total_seconds=time.time() - t_all)
+             factors=np.array(args.factors), fine=np.array(info["fine"]), clip=clip.cpu().numpy())
+    report = dict(closure="dimensionless: x = (g/|G|, min(z_w/Delta, 16), z_w/h), tau = (Delta |G|)^2 c",
+                  data=info, clip=clip.cpu().numpy().tolist(),
+                  training=dict(steps=steps, seconds=secs, batch=args.batch, lr=args.lr, epochs=args.epochs,
+                                samples=nsamples, samples_per_s=steps * args.batch / max(secs, 1e-9),
+                                loss=hist[::max(1, len(hist) // 50)] + hist[-1:]),
+                  apriori_heldout=rep_ho, total_seconds=time.time() - t_all)
     with open(args.out + ".json", "w") as fh:
         json.dump(report, fh, indent=1)
     log(json.dumps(rep_ho, indent=1))
     return report
 
 
-def evaluate(args, log=print):
-    """A-posteriori runs only, from <out>.npz (network) and <out>_eval.npz
-    (first filtered snapshot and the filtered fine run's mean profile);
-    updates the 'aposteriori' entry of <out>.json."""
-    z = np.load(args.out + ".npz")
-    ev = np.load(args.out + "_eval.npz")
-    info = json.loads(str(ev["meta"]))
-    apost = aposteriori(ev["first"], info, z["params"], z["norm"], args.aposteriori or 4000, log,
-                        getattr(args, "guard", 0.0))
-    rp = args.out + ".json"
-    rep_ = json.load(open(rp)) if os.path.exists(rp) else {}
-    rep_["aposteriori"] = apost
-    with open(rp, "w") as fh:
-        json.dump(rep_, fh, indent=1)
-    return apost
-
-
 def main(argv=None):
     ap = argparse.ArgumentParser(description="Train the learned SGS closure on one GPU.")
     ap.add_argument("--fine", type=int, nargs=3, default=[384, 384, 192])
-    ap.add_argument("--factor", type=int, nargs=2, default=[4, 2])
+    ap.add_argument("--factors", type=int, nargs="+", default=[2, 4],
+                    help="filter factors f: coarse grids (nx/f, ny/f, nz/f); f = 1 or even")
     ap.add_argument("--re-tau", type=float, default=395.0)
-    ap.add_argument("--snapshots", type=int, default=200)
+    ap.add_argument("--snapshots", type=int, default=100)
     ap.add_argument("--spinup", type=int, default=14000)
     ap.add_argument("--spinup-precision", type=int, choices=[4, 8], default=4)
-    ap.add_argument("--every", type=int, default=40)
+    ap.add_argument("--every", type=int, default=60)
     ap.add_argument("--amp", type=float, default=1.0)
     ap.add_argument("--large", type=float, default=0.3)
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--holdout", type=float, default=0.1)
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--aposteriori", type=int, default=0, help="coarse steps of the a-posteriori runs (0 = skip)")
-    ap.add_argument("--guard", type=float, default=0.0,
-                    help="fallback factor against the Deardorff dissipation in the a-posteriori learned run "
-                         "(0 = sign test only: the network itself is judged)")
     ap.add_argument("--resolved-only", action="store_true",
                     help="targets without the fine run's own model stress")
     ap.add_argument("--out", default=os.path.join(HERE, "weights", "sgs_c4"))
-    ap.add_argument("--evaluate", action="store_true",
-                    help="only the a-posteriori runs, from <out>.npz and <out>_eval.npz")
-    args = ap.parse_args(argv)
-    if args.evaluate:
-        evaluate(args)
-    else:
-        run(args)
+    run(ap.parse_args(argv))
 
 
 if __name__ == "__main__":

@@ -23,22 +23,22 @@ def make_case(sign):
     cfg.dt = o.dt_used
     fl = o.get_fields()
     P = O.mlp_init(seed=31)
-    N = np.concatenate([np.zeros(11), np.full(9, 30.0), [2.0 / RE_TAU, 0.0], np.full(6, sign * 1e-3), np.zeros(6)])
+    N = np.concatenate([np.zeros(11), np.full(9, 3.0), [0.2, 2.0], np.full(6, sign * 0.02), np.zeros(6)])
     return cfg, o, fl, P, N
 
 
 def np_learned(cfg, fl, P, N):
     u, v, w = fl["u"], fl["v"], fl["w"]
-    f = LN.features(u, v, w, cfg.xl, cfg.yl, cfg.zl, RE_TAU)
+    f, sc = LN.features(u, v, w, cfg.xl, cfg.yl, cfg.zl)
     y = LN.mlp(P, (f - N[:11]) * N[11:22])
-    tau = (y * N[22:28] + N[28:34]).T.reshape(6, NZ, NY, NX)
+    tau = ((y * N[22:28] + N[28:34]) * (sc ** 2)[:, None]).T.reshape(6, NZ, NY, NX)
     g = LN.gradients(u, v, w, cfg.xl, cfg.yl, cfg.zl)
     dz = cfg.zl / NZ
     xkmax = dz * dz / cfg.dt / 5.0
     nut = LN.network_viscosity(g, tau, xkmax)
     dsl = (cfg.xl / NX * cfg.yl / NY * dz) ** (1.0 / 3.0)
-    dis_d = LN.deardorff_dissipation(g, fl["e"], dsl, xkmax)
-    return LN.dissipation(g, tau), dis_d, LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl, u, v, nut)
+    dis_r = LN.reference_dissipation(g, dsl)
+    return LN.dissipation(g, tau), dis_r, LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl, u, v, nut)
 
 
 @pytest.mark.parametrize("guard", [0.0, 4.0, 1e6])
@@ -49,10 +49,10 @@ def test_learned_prepare_matches_numpy(sign, guard):
     o.set_learned_guard(guard)
     o.stage(0, 0, 1)
     used, dis = o.learned_status()
-    dis_np, dis_d_np, (lru, lrv, lrw) = np_learned(cfg, fl, P, N)
+    dis_np, dis_r_np, (lru, lrv, lrw) = np_learned(cfg, fl, P, N)
     assert abs(dis - dis_np) <= 1e-9 * abs(dis_np)
-    assert abs(o.learned_deardorff() - dis_d_np) <= 1e-9 * abs(dis_d_np) and dis_d_np > 0
-    assert used == LN.network_used(dis_np, dis_d_np, guard)
+    assert abs(o.learned_reference() - dis_r_np) <= 1e-9 * abs(dis_r_np) and dis_r_np > 0
+    assert used == LN.network_used(dis_np, dis_r_np, guard)
     if used:
         a, b, c = o.learned_divergence()
         for x, y in ((a, lru), (b, lrv), (c, lrw)):
@@ -124,3 +124,20 @@ def test_filter_constants_and_z_box():
     u = np.broadcast_to(uz[:, None, None], (nz, ny, nx)).copy()
     out = LN.filter_fields(u, v, w, xl, yl, 4, 2)
     np.testing.assert_allclose(out[3][:, 0, 0], 0.25 * (uz[0::2] - uz[1::2]) ** 2, rtol=1e-12)
+
+
+@pytest.mark.parametrize("fz", [2, 4])
+def test_filter_z_box_of_w_is_exact_for_linear_profiles(fz):
+    """w at the coarse faces: the trapezoid box of fz fine cells centred on
+    the face reproduces a w that is linear in z (away from the top wall,
+    where w(nz) = 0 breaks the line)."""
+    nx, ny, nz, xl, yl, zl = 16, 16, 16, 2 * np.pi, np.pi, 2.0
+    k = np.arange(1, nz + 1, dtype=np.float64)
+    w = np.broadcast_to((0.3 + 0.05 * k)[:, None, None], (nz, ny, nx)).copy()
+    w[-1] = 0.0
+    u = np.zeros_like(w)
+    out = LN.filter_fields(u, u, w, xl, yl, 4, fz)
+    nzc = nz // fz
+    for K in range(1, nzc):
+        if fz * K + fz // 2 <= nz - 1:
+            np.testing.assert_allclose(out[2][K - 1], 0.3 + 0.05 * fz * K, rtol=1e-13)
