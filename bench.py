@@ -447,6 +447,18 @@ def main():
             if len(f) >= 3 and f[0] == kname:
                 traffic = float(f[2])
     stage_ms = sum(t for _, t in prof)
+    # compute roof of the fused row kernel: its transform and pointwise flops
+    # (12 complex transforms of 3nx/2 points at 5 N log2 N, ~150 flops per
+    # point of the pointwise rows) per padded row and level, against the
+    # device's FP32 / FP64 FMA rate from the library's probe kernel
+    mxp = 3 * NX // 2
+    row_flops = 3 * NY // 2 * NZ * (12 * 5.0 * mxp * np.log2(mxp) + 150.0 * mxp)
+    fma32, fma64 = P.fma_rate(4, dev), P.fma_rate(8, dev)
+    def compute_roof(profile, peak):
+        ms = sum(t for n, t in profile if n.startswith("k_row_fused"))
+        return {"kernel": "k_row_fused", "flops_per_launch": row_flops, "kernel_ms": ms,
+                "achieved_tflops": row_flops / (ms / 1e3) / 1e12, "peak_tflops": peak / 1e12,
+                "frac": row_flops / (ms / 1e3) / peak, "peak_source": "les_probe_fma_rate (measured FMA rate)"}
     # the network's tensor-core kernel: 2*(11*64 + 2*64*64 + 64*6) flops per point
     fpp = 2 * (11 * 64 + 2 * 64 * 64 + 64 * 6)
     mlp_ms = sum(t for n, t in prof if n.startswith("k_mlp_infer"))
@@ -489,6 +501,8 @@ def main():
         "roofline_network": {"bound": "tensor", "kernel": "k_mlp_infer", "achieved": mlp_tf, "peak": bf16_peak,
                              "unit": "TFLOP/s", "frac": (mlp_tf / bf16_peak) if mlp_tf else None,
                              "kernel_ms": mlp_ms, "flops_per_point": fpp, "peak_source": bf16_kind},
+        "roofline_compute": {"learned_mixed_f32": compute_roof(prof, fma32), "mixed_f32": compute_roof(prof32, fma32),
+                             "fp64": compute_roof(prof64, fma64)},
         "kernels_ms_stage2_learned_mixed": {n: round(t, 4) for n, t in prof},
         "kernels_ms_stage2_fp64": {n: round(t, 4) for n, t in prof64},
         "kernels_ms_stage2_mixed": {n: round(t, 4) for n, t in prof32},

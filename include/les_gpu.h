@@ -263,6 +263,14 @@ int les_gpu_field_wait(les_handle* h);
 int les_gpu_read_field(les_handle* h, const char* path, int real_bytes, double* time);
 int les_gpu_field_header(const char* path, int real_bytes, int* dims, double* hdr);
 
+/* Measurement helper with no counterpart in the reference: the device's
+ * vector fused-multiply-add rate in flop/s for real_bytes = 4 (FP32) or 8
+ * (FP64), timed by this library's own kernel (8 independent FMA chains per
+ * thread, 16 CTAs of 256 threads per SM, CUDA events after a warm-up,
+ * about 0.1 s).  It is the compute roof the FP32 / FP64 transform kernels
+ * are read against.  Synchronous; allocates 8 bytes of device memory. */
+int les_probe_fma_rate(int real_bytes, int device, double* flops_per_s);
+
 /* Message of the last failed les_op_* call on this thread. */
 const char* les_op_last_error(void);
 

@@ -121,6 +121,7 @@ def lib():
         "les_op_deal": (I, [VP, I, I, I, I, VP]),
         "les_op_tridv": (I, [VP, I, I, I, VP]),
         "les_op_last_error": (ctypes.c_char_p, []),
+        "les_probe_fma_rate": (I, [I, I, ctypes.POINTER(D)]),
         # learned closure (les_mlp.h)
         "les_mlp_create": (I, [I, ctypes.POINTER(VP)]),
         "les_mlp_destroy": (None, [VP]),
@@ -608,3 +609,12 @@ def field_header(path, real_bytes=8):
         raise LesError(rc, lib().les_gpu_last_error(None).decode())
     keys = ("time", "xl", "yl", "zl", "dt", "z0", "utau", "divgls", "fcor", "ugtop", "ugbot", "vgtop", "vgbot")
     return tuple(dims), dict(zip(keys, list(hdr)))
+
+
+def fma_rate(real_bytes, device=0):
+    """Vector FMA throughput of the device in flop/s (les_probe_fma_rate)."""
+    r = ctypes.c_double()
+    rc = lib().les_probe_fma_rate(real_bytes, device, ctypes.byref(r))
+    if rc != LES_OK:
+        raise LesError(rc, "les_probe_fma_rate failed")
+    return r.value

@@ -61,3 +61,13 @@ def test_tridv_matches_oracle(gpu_lib, product):
     got = product.tridv(torch.tensor(bd, device="cuda")).cpu().numpy()
     np.testing.assert_allclose(got[3], ref[3], rtol=1e-13, atol=1e-13 * np.abs(ref[3]).max())
     np.testing.assert_allclose(got[1], ref[1], rtol=1e-14)
+
+
+def test_fma_probe_rates(gpu_lib, product):
+    """The compute roof of the transform kernels: the device's vector FMA
+    rate from the library's own probe kernel, FP32 above FP64, both above
+    1 TFLOP/s (a B200 delivers tens)."""
+    f32 = product.fma_rate(4)
+    f64 = product.fma_rate(8)
+    assert f32 > 1e12 and f64 > 1e12
+    assert f32 > f64
