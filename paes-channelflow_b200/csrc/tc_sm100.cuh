@@ -119,11 +119,26 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// Non-blocking test of phase `parity` (mbarrier.try_wait may suspend the
+// thread for a while before it reports an incomplete phase; test_wait never
+// does).
+__device__ __forceinline__ uint32_t mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok;
+}
 // Wait for phase `parity` of the barrier to complete; gives up once limit_ns
 // nanoseconds have passed since the first unsuccessful poll and returns
-// false (limit 0: at the second unsuccessful poll).
+// false.  Limit 0 gives up at once when the first (non-blocking) poll finds
+// the phase incomplete.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
-  if (mbar_try(bar, parity)) return true;
+  if (mbar_test(bar, parity)) return true;
+  if (limit_ns == 0) return false;
   const uint64_t t0 = globaltimer_ns();
   while (!mbar_try(bar, parity)) {
     if (globaltimer_ns() - t0 >= limit_ns) return false;
