@@ -9,7 +9,7 @@
  * imodel = LES_SGS_LEARNED (les_gpu.h) and a network is attached with
  * les_gpu_set_mlp; stages whose mean dissipation -<tau_ij S_ij> comes out
  * negative, or (les_gpu_set_learned_guard) outside a factor of the
- * Smagorinsky estimate, fall back to the Deardorff stresses.
+ * Smagorinsky-Lilly estimate, fall back to the Deardorff stresses.
  *
  * Network: 11 -> 64 -> 64 -> 64 -> 6, GELU (tanh form) after the hidden
  * layers, bf16 weights and activations, f32 accumulation.  The closure is
@@ -97,15 +97,21 @@ int les_mlp_adam_step(les_mlp* m, const void* feat, const float* target, long lo
 int les_gpu_set_mlp(les_handle* h, les_mlp* m, double re_tau);
 
 /* After a synchronising call: 1 if the last stage used the network (0 if
- * it fell back to the Deardorff stresses) and that stage's plane-averaged
- * dissipation -<tau_ij S_ij> of the network's stresses. */
+ * it fell back to the Deardorff stresses) and that stage's mean
+ * dissipation -<tau'_ij S_ij> of the applied (projected) stresses. */
 int les_gpu_learned_status(les_handle* h, int* used, double* dissipation);
 
-/* The fallback test of each stage: the network is used when its mean
- * dissipation -<tau_ij S_ij> is >= 0 (the spec'd test) and, with
- * ratio > 0, within a factor ratio of the reference dissipation
- * <(0.1 Delta)^2 |S|^3>, the Smagorinsky estimate with the constant of the
- * reference's imodel 4 (complen.f90:22-23), |S| = (2 S_ij S_ij)^(1/2), on
+/* The stress the solver applies is the network's with its local
+ * backscatter removed: where tau_ij S_ij > 0 (energy flowing from the
+ * sub-filter to the resolved scales) the component along S is subtracted,
+ * tau' = tau - (tau:S / S:S) S, so the applied stress never injects energy
+ * at a point.
+ *
+ * The fallback test of each stage: the network is used when the mean
+ * dissipation -<tau_ij S_ij> of its raw prediction is >= 0 (the spec'd
+ * test) and, with ratio > 0, the applied mean -<tau'_ij S_ij> lies within a
+ * factor ratio of the reference <(C_s Delta)^2 |S|^3>, the Smagorinsky
+ * estimate with Lilly's constant C_s = 0.17, |S| = (2 S_ij S_ij)^(1/2), on
  * the same state.  The second test keeps a network out of states whose
  * sub-filter dissipation it would misjudge by more than that factor.
  * Default ratio 4; ratio <= 0 disables it.  Drops the handle's captured

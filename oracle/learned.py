@@ -120,21 +120,34 @@ def dissipation(g, tau):
     return float(d.mean())
 
 
-def reference_dissipation(g, dsl):
-    """Mean of (0.1 dsl)^2 |S|^3 over all cell centres, |S|^2 = 2 S_ij S_ij:
-    the Smagorinsky estimate with the constant of complen.f90:22-23."""
+def project_backscatter(g, tau):
+    """Remove local backscatter: where tau:S > 0 the stress's component
+    along S is subtracted, tau' = tau - (tau:S / S:S) S, so -tau':S =
+    max(-tau:S, 0) at every point.  g from gradients(), tau (6, ...)."""
+    S = [g[0], g[4], g[8], 0.5 * (g[3] + g[1]), 0.5 * (g[6] + g[2]), 0.5 * (g[7] + g[5])]
+    w = [1.0, 1.0, 1.0, 2.0, 2.0, 2.0]
+    ts = sum(w[i] * tau[i] * S[i] for i in range(6))
+    ss = sum(w[i] * S[i] * S[i] for i in range(6))
+    a = np.where((ts > 0) & (ss > 0), -ts / np.where(ss > 0, ss, 1.0), 0.0)
+    return np.stack([tau[i] + a * S[i] for i in range(6)])
+
+
+def reference_dissipation(g, dsl, cs=0.17):
+    """Mean of (cs dsl)^2 |S|^3 over all cell centres, |S|^2 = 2 S_ij S_ij:
+    the Smagorinsky estimate with Lilly's constant."""
     s11, s22, s33 = g[0], g[4], g[8]
     s12, s13, s23 = 0.5 * (g[3] + g[1]), 0.5 * (g[6] + g[2]), 0.5 * (g[7] + g[5])
     ss = 2 * (s11 ** 2 + s22 ** 2 + s33 ** 2 + 2 * (s12 ** 2 + s13 ** 2 + s23 ** 2))
-    return float((0.01 * dsl * dsl * ss * np.sqrt(ss)).mean())
+    return float((cs * cs * dsl * dsl * ss * np.sqrt(ss)).mean())
 
 
-def network_used(dis, dis_r, guard):
-    """The stage's fallback rule: the network's mean dissipation must be
-    >= 0 and, with guard > 0, within a factor guard of the reference's."""
-    if not dis >= 0:
+def network_used(dis_raw, dis_applied, dis_r, guard):
+    """The stage's fallback rule: the raw network's mean dissipation must be
+    >= 0 and, with guard > 0, the applied one within a factor guard of the
+    reference's."""
+    if not dis_raw >= 0:
         return 0
-    if guard > 0 and not (dis_r > 0 and dis <= guard * dis_r and guard * dis >= dis_r):
+    if guard > 0 and not (dis_r > 0 and dis_applied <= guard * dis_r and guard * dis_applied >= dis_r):
         return 0
     return 1
 

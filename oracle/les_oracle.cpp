@@ -351,7 +351,7 @@ struct Les {
   // factor `learned_guard` of the reference (Smagorinsky) dissipation on the
   // same state (learned_guard <= 0: only the sign test)
   double learned_guard = 4.0;
-  double learned_dissip_r = 0.0;
+  double learned_dissip_r = 0.0, learned_dissip_raw = 0.0;
   long long learned_stages = 0, learned_stages_used = 0;
   T sgs_mom = (T)1;  // weight of the interior momentum stresses of compsgs1
   Levels<T> lru, lrv, lrw;
@@ -766,11 +766,13 @@ struct Les {
   //   one-sided at k = 1 and nnz (derivs1.f90 / derivs2.f90 wall rows);
   // dimensionless features (g / |G|, min(z_w / dsl, 16), z_w / h),
   // normalised, through the FP64 network; tau = (dsl |G|)^2 c with c the
-  // de-normalised outputs; the stage uses the network when the mean of
-  // -tau_ij S_ij is >= 0 and, with learned_guard > 0, within a factor
-  // learned_guard of the reference mean dissipation (0.1 dsl)^2 |S|^3
-  // (|S|^2 = 2 S_ij S_ij; the Smagorinsky estimate with complen.f90:22-23's
-  // constant), and then adds the dealiased stress divergence to ru, rv, rw:
+  // de-normalised outputs, and where tau:S > 0 (local backscatter) the
+  // component along S removed: tau' = tau - (tau:S / S:S) S.  The stage
+  // uses the network when the raw mean of -tau_ij S_ij is >= 0 and, with
+  // learned_guard > 0, the applied mean -tau':S lies within a factor
+  // learned_guard of the reference mean dissipation (C_s dsl)^2 |S|^3
+  // (|S|^2 = 2 S_ij S_ij; Lilly's constant C_s = 0.17), and then adds the
+  // dealiased stress divergence of tau' to ru, rv, rw:
   //   ru += -d/dx tau11 - d/dy tau12 - (tau13w(k) - tau13w(k-1))/dz, ...
   // with tau13w(k) = (tau13(k) + tau13(k+1))/2 on the interior w-levels and 0
   // on the walls (the wall model's stresses stay in compsgs1), plus the
@@ -782,7 +784,7 @@ struct Les {
     std::vector<std::vector<T>> g(9, std::vector<T>(ps));
     std::vector<T> wc(ps);
     const double h = (double)zl / 2.0;
-    double dsum_ = 0.0, dsumr_ = 0.0;
+    double dsum_ = 0.0, dsumr_ = 0.0, dsumraw_ = 0.0;
     std::vector<double> nuA((size_t)NZ + 2, 0.0), nuB((size_t)NZ + 2, 0.0);
     for (int iz = 1; iz <= NZ; iz++) {
       sp.xderiv(u.at(iz), g[0].data(), xk.data(), nnx, nny);
@@ -819,23 +821,28 @@ struct Les {
         mlp_forward(mlpP.data(), x, tr, mlp_bf16);
         const double sc = gm * (double)dsl, sc2 = sc * sc;
         double t[kOut];
-        for (int o = 0; o < kOut; o++) {
-          t[o] = sc2 * (tr.y[o] * mlpN[2 * kIn + o] + mlpN[2 * kIn + kOut + o]);
-          TA(o, iz)[q] = (T)t[o];
+        for (int o = 0; o < kOut; o++) t[o] = sc2 * (tr.y[o] * mlpN[2 * kIn + o] + mlpN[2 * kIn + kOut + o]);
+        const double sv[6] = {(double)g[0][q], (double)g[4][q], (double)g[8][q], 0.5 * ((double)g[3][q] + g[1][q]),
+                              0.5 * ((double)g[6][q] + g[2][q]), 0.5 * ((double)g[7][q] + g[5][q])};
+        const double sS = sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2] + 2.0 * (sv[3] * sv[3] + sv[4] * sv[4] + sv[5] * sv[5]);
+        const double tS = t[0] * sv[0] + t[1] * sv[1] + t[2] * sv[2] + 2.0 * (t[3] * sv[3] + t[4] * sv[4] + t[5] * sv[5]);
+        dsumraw_ += -tS;
+        if (tS > 0.0 && sS > 0.0) {
+          for (int o = 0; o < kOut; o++) t[o] -= tS / sS * sv[o];
+        } else {
+          dsum_ += -tS;
         }
-        const double s11 = g[0][q], s22 = g[4][q], s33 = g[8][q];
-        const double s12 = 0.5 * ((double)g[3][q] + g[1][q]), s13 = 0.5 * ((double)g[6][q] + g[2][q]),
-                     s23 = 0.5 * ((double)g[7][q] + g[5][q]);
-        dsum_ += -(t[0] * s11 + t[1] * s22 + t[2] * s33 + 2.0 * (t[3] * s12 + t[4] * s13 + t[5] * s23));
-        const double ss = 2.0 * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23));
-        dsumr_ += 0.01 * (double)dsl * (double)dsl * ss * std::sqrt(ss);
+        for (int o = 0; o < kOut; o++) TA(o, iz)[q] = (T)t[o];
+        const double ss = 2.0 * sS;  // |S|^2
+        dsumr_ += 0.17 * 0.17 * (double)dsl * (double)dsl * ss * std::sqrt(ss);
         nuA[iz] += t[4] * (double)g[6][q] + t[5] * (double)g[7][q];
         nuB[iz] += (double)g[6][q] * g[6][q] + (double)g[7][q] * g[7][q];
       }
     }
     learned_dissip = dsum_ / ((double)ps * NZ);
     learned_dissip_r = dsumr_ / ((double)ps * NZ);
-    learned_used = learned_dissip >= 0.0 ? 1 : 0;  // NaN -> fallback
+    learned_dissip_raw = dsumraw_ / ((double)ps * NZ);
+    learned_used = learned_dissip_raw >= 0.0 ? 1 : 0;  // NaN -> fallback
     if (learned_guard > 0.0 && !(learned_dissip_r > 0.0 && learned_dissip <= learned_guard * learned_dissip_r &&
                                  learned_guard * learned_dissip >= learned_dissip_r))
       learned_used = 0;
@@ -1313,6 +1320,14 @@ int orc_get_learned(void* hp, double* lru, double* lrv, double* lrw) {
 void orc_learned_status(void* hp, int* used, double* dissipation) {
   OrcHandle* h = (OrcHandle*)hp;
   DISPATCH(h, { if (used) *used = L.learned_used; if (dissipation) *dissipation = L.learned_dissip; });
+}
+// Raw network mean dissipation (before the backscatter projection) of the
+// last learned stage.
+double orc_learned_raw(void* hp) {
+  OrcHandle* h = (OrcHandle*)hp;
+  double d = 0.0;
+  DISPATCH(h, { d = L.learned_dissip_raw; });
+  return d;
 }
 // Reference (Smagorinsky) mean dissipation of the last learned stage.
 double orc_learned_reference(void* hp) {

@@ -116,6 +116,8 @@ def lib():
         L.orc_learned_status.argtypes = [P, ctypes.POINTER(ctypes.c_int), D]
         L.orc_learned_reference.argtypes = [P]
         L.orc_learned_reference.restype = ctypes.c_double
+        L.orc_learned_raw.argtypes = [P]
+        L.orc_learned_raw.restype = ctypes.c_double
         L.orc_set_learned_guard.argtypes = [P, ctypes.c_double]
         L.orc_get_learned.argtypes = [P, D, D, D]
         L.orc_bf16_round.restype = ctypes.c_double
@@ -219,6 +221,11 @@ class Oracle:
         d = np.zeros(1)
         lib().orc_learned_status(self.h, ctypes.byref(used), _ptr(d))
         return used.value, float(d[0])
+
+    def learned_raw(self):
+        """Raw network mean dissipation (before the backscatter projection)
+        of the last learned stage."""
+        return float(lib().orc_learned_raw(self.h))
 
     def learned_reference(self):
         """Reference (Smagorinsky) mean dissipation of the last learned stage."""

@@ -73,6 +73,23 @@ def run(P, grid, re_tau, precision, imodel, steps, every, dt=None, mlp=None, gua
     return out, counts, dt
 
 
+def averaged(prof, ref, steps):
+    """Profiles averaged over the checkpoints of the second half of the run
+    (a statistical comparison: the instantaneous fields of two turbulent
+    runs decorrelate once round-off differences have grown)."""
+    keys = [it for it in sorted(prof) if it > steps // 2 and it in ref]
+    if not keys:
+        return {}
+    avg = lambda d, j: np.mean([d[it][j] for it in keys], axis=0)
+    U, uw, ur = avg(prof, 0), avg(prof, 1), avg(prof, 2)
+    U0, uw0, ur0 = avg(ref, 0), avg(ref, 1), avg(ref, 2)
+    ub = float(np.mean(U0))
+    return {"checkpoints": len(keys), "from_step": keys[0], "to_step": keys[-1],
+            "mean_u_max_err_over_ub": float(np.abs(U - U0).max() / ub),
+            "uw_max_err_over_max": float(np.abs(uw - uw0).max() / max(np.abs(uw0).max(), 1e-300)),
+            "u_rms_max_err_over_max": float(np.abs(ur - ur0).max() / max(ur0.max(), 1e-300))}
+
+
 def compare(prof, ref, counts, dt, nx):
     rows = []
     kmax = nx // 3
@@ -102,7 +119,8 @@ def main(argv=None):
     ap.add_argument("--re-tau", type=float, default=590.0)
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--every", type=int, default=500)
-    ap.add_argument("--forms", default="mixed,learned,learned_sign_only")
+    ap.add_argument("--forms", default="mixed,learned,learned_sign_only",
+                    help="comma list of mixed, learned, learned_sign_only, learned_guard<factor>")
     ap.add_argument("--weights", default=os.path.join(HERE, "weights", "sgs_c4.npz"))
     ap.add_argument("--out", default="aposteriori.json")
     a = ap.parse_args(argv)
@@ -126,9 +144,13 @@ def main(argv=None):
                 r = run(P, a.grid, a.re_tau, P.PREC_MIXED, P.SGS_LEARNED, a.steps, a.every, dt, mlp)
             elif name == "learned_sign_only":
                 r = run(P, a.grid, a.re_tau, P.PREC_MIXED, P.SGS_LEARNED, a.steps, a.every, dt, mlp, 0.0)
+            elif name.startswith("learned_guard"):
+                r = run(P, a.grid, a.re_tau, P.PREC_MIXED, P.SGS_LEARNED, a.steps, a.every, dt, mlp,
+                        float(name[len("learned_guard"):]))
             else:
                 raise ValueError(name)
             res["forms"][name] = compare(r[0], ref, r[1], dt, a.grid[0])
+            res.setdefault("second_half_average", {})[name] = averaged(r[0], ref, a.steps)
         except P.LesError as e:  # e.g. a run that blew up (LES_ENAN): recorded, the others still run
             res["forms"][name] = {"failed": str(e)}
         with open(a.out, "w") as f:
@@ -136,6 +158,8 @@ def main(argv=None):
     for name, rows in res["forms"].items():
         for r in (rows if isinstance(rows, list) else [rows]):
             print(name, json.dumps(r))
+    for name, r in res.get("second_half_average", {}).items():
+        print("second-half average", name, json.dumps(r))
 
 
 if __name__ == "__main__":

@@ -282,7 +282,7 @@ struct Engine : EngineBase {
     clipflag.release(); ephys.release(); dEX.release(); dEY.release(); wallpl.release();
     for (auto& b : xout) b.release();
     for (auto& b : phys) b.release();
-    lgy.release(); ltau.release(); lfeat.release(); fraw.release(); lpart.release(); lnut.release(); lstat.release(); lflag.release();
+    lgy.release(); ltau.release(); lfeat.release(); fraw.release(); lpart.release(); lnut.release(); lstat.release(); lflag.release(); lcount.release();
     fscr.release(); fcp.release(); fsh.release(); fch.release();
   }
   cudaStream_t stream() override { return st; }
@@ -500,9 +500,9 @@ struct Engine : EngineBase {
     lgy.alloc(6 * nm * NZ);
     ltau.alloc(8 * ps * NZ);
     lfeat.alloc(2 * ps * NZ);
-    lpart.alloc((size_t)2 * nsm * kInferCtasPerSm);  // per-CTA pairs: network, reference
+    lpart.alloc((size_t)3 * nsm * kInferCtasPerSm);  // per-CTA triples: raw, applied, reference
     lnut.alloc((size_t)NZ * kNuChunks * 2 + NZ + 1);  // partial sums, then the face values
-    lstat.alloc(3);
+    lstat.alloc(4);
     lcount.alloc(2);
     lflag.alloc(1);
   }

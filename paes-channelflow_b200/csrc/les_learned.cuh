@@ -25,13 +25,14 @@
 //      (an eddy viscosity is the special case c = -2 C^2 (|S|/|G|) S/|G|);
 //      Delta |G| rides along in bf16 columns 11 (high part) and 12 (the
 //      rounding remainder), which the network's padded first layer ignores;
-//   3. k_mlp_infer<MlpOutTau>: tau_ij on the tensor cores, and per CTA the
-//      sums of the network's dissipation -tau_ij S_ij and of the reference
-//      dissipation (0.1 Delta)^2 |S|^3 (the Smagorinsky estimate with the
-//      reference's imodel 4 constants, complen.f90:22-23);
+//   3. k_mlp_infer<MlpOutTau>: tau_ij on the tensor cores with its local
+//      backscatter removed (the component along S where tau:S > 0), and
+//      per CTA the sums of the raw network's dissipation -tau_ij S_ij, of
+//      the applied one and of the reference (C_s Delta)^2 |S|^3 (the
+//      Smagorinsky estimate with Lilly's constant C_s = 0.17);
 //   4. k_learned_flag: the means (FP64, fixed order); flag = 1 when the
-//      network's is >= 0 and (guard > 0) within a factor guard of the
-//      reference's, else 0 (Deardorff fallback);
+//      raw network's is >= 0 and (guard > 0) the applied one lies within a
+//      factor guard of the reference, else 0 (Deardorff fallback);
 //   ... the padded-grid kernels (their interior momentum stresses are
 //      multiplied by 1 - flag) ...
 //   5. k_row_r2c + k_col_small: tau^ at every level;
@@ -209,60 +210,78 @@ __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 
 // Delta |G| from the bf16 columns 11 (high part) and 12 (remainder).
 __device__ __forceinline__ float feat_scale(uint4 f1) { return bf_hi(f1.y) + bf_lo(f1.z); }
 
+// Squared constant of the reference dissipation (C_s Delta)^2 |S|^3 of the
+// fallback test: Lilly's inertial-range Smagorinsky constant C_s = 0.17.
+constexpr double kRefCs2 = 0.17 * 0.17;
+
 // Network outputs -> tau planes [6][N] (tau11, tau22, tau33, tau12, tau13,
-// tau23) = (Delta |G|)^2 (y * out_scale + out_shift); planes 6, 7:
-// tau13 g_uz + tau23 g_vz and g_uz^2 + g_vz^2 (g = the gradients times
-// Delta, for the network's effective viscosity); returns the network's
-// dissipation -tau_ij S_ij and the reference (0.1 Delta)^2 |S|^3, each
-// times Delta (k_learned_flag divides the sums by N Delta).
+// tau23).  The network's stress is tau = (Delta |G|)^2 (y * out_scale +
+// out_shift); where it would transfer energy from the sub-filter scales to
+// the resolved ones (tau_ij S_ij > 0, local backscatter) its component
+// along S is removed, tau' = tau - (tau:S / S:S) S, so that the applied
+// stress never injects energy at a point (-tau':S = max(-tau:S, 0)).
+// Planes 6, 7: tau13' g_uz + tau23' g_vz and g_uz^2 + g_vz^2 (g = the
+// gradients times Delta, for the network's effective viscosity).  Returns,
+// each times Delta (k_learned_flag divides the sums by N Delta): the raw
+// network's dissipation -tau:S, the applied -tau':S, and the reference
+// (C_s Delta)^2 |S|^3.
 template <class T> struct MlpOutTau {
   T* tau;  // [8][N]
   long long N;
-  __device__ double2 operator()(long long p, bool valid, const float (&y)[16], uint4 f0, uint4 f1,
+  __device__ double3 operator()(long long p, bool valid, const float (&y)[16], uint4 f0, uint4 f1,
                                 const MlpDev* P) const {
-    if (!valid) return make_double2(0.0, 0.0);
+    if (!valid) return make_double3(0.0, 0.0, 0.0);
     const float s = feat_scale(f1);
     const float s2 = s * s;
     float t[6];
 #pragma unroll
-    for (int i = 0; i < 6; i++) {
-      t[i] = s2 * (y[i] * P->out_scale[i] + P->out_shift[i]);
-      tau[(size_t)i * N + p] = (T)t[i];
-    }
+    for (int i = 0; i < 6; i++) t[i] = s2 * (y[i] * P->out_scale[i] + P->out_shift[i]);
     const float q[9] = {bf_lo(f0.x), bf_hi(f0.x), bf_lo(f0.y), bf_hi(f0.y), bf_lo(f0.z),
                         bf_hi(f0.z), bf_lo(f0.w), bf_hi(f0.w), bf_lo(f1.x)};
     float g[9];
 #pragma unroll
     for (int j = 0; j < 9; j++) g[j] = (q[j] * P->in_rscale[j] + P->in_shift[j]) * s;  // d_i u_j * Delta
+    const float sv[6] = {g[0], g[4], g[8], 0.5f * (g[3] + g[1]), 0.5f * (g[6] + g[2]), 0.5f * (g[7] + g[5])};
+    const double ss = (double)sv[0] * sv[0] + (double)sv[1] * sv[1] + (double)sv[2] * sv[2] +
+                      2.0 * ((double)sv[3] * sv[3] + (double)sv[4] * sv[4] + (double)sv[5] * sv[5]);  // S:S
+    const double ts = (double)t[0] * sv[0] + (double)t[1] * sv[1] + (double)t[2] * sv[2] +
+                      2.0 * ((double)t[3] * sv[3] + (double)t[4] * sv[4] + (double)t[5] * sv[5]);  // tau:S
+    double applied = -ts;
+    if (ts > 0.0 && ss > 0.0) {
+      const float a = (float)(-ts / ss);
+#pragma unroll
+      for (int i = 0; i < 6; i++) t[i] += a * sv[i];
+      applied = 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < 6; i++) tau[(size_t)i * N + p] = (T)t[i];
     tau[(size_t)6 * N + p] = (T)(t[4] * g[6] + t[5] * g[7]);
     tau[(size_t)7 * N + p] = (T)(g[6] * g[6] + g[7] * g[7]);
-    const float s11 = g[0], s22 = g[4], s33 = g[8];
-    const float s12 = 0.5f * (g[3] + g[1]), s13 = 0.5f * (g[6] + g[2]), s23 = 0.5f * (g[7] + g[5]);
-    const double ss = 2.0 * ((double)s11 * s11 + (double)s22 * s22 + (double)s33 * s33 +
-                             2.0 * ((double)s12 * s12 + (double)s13 * s13 + (double)s23 * s23));  // (|S| Delta)^2
-    const double net = -((double)t[0] * s11 + (double)t[1] * s22 + (double)t[2] * s33 +
-                         2.0 * ((double)t[3] * s12 + (double)t[4] * s13 + (double)t[5] * s23));
-    return make_double2(net, 0.01 * ss * sqrt(ss));
+    const double sm2 = 2.0 * ss;  // (|S| Delta)^2
+    return make_double3(-ts, applied, kRefCs2 * sm2 * sqrt(sm2));
   }
 };
 
-// Mean dissipations (per-CTA pairs of sums in CTA order: the network's,
-// the reference's) -> flag, status [network mean, flag, reference mean] and
-// the stage counters [stages, stages that used the network].  guard <= 0:
-// the sign test only.
+// Mean dissipations (per-CTA triples of sums in CTA order: the raw
+// network's, the applied, the reference) -> flag, status [applied mean,
+// flag, reference mean, raw mean] and the stage counters [stages, stages
+// that used the network].  The network is used when its raw mean
+// dissipation is >= 0 (NaN falls back) and, with guard > 0, the applied
+// mean lies within a factor guard of the reference.
 static __global__ void k_learned_flag(const double* __restrict__ part, int nparts, double inv_n_delta, double guard,
                                       int* __restrict__ flag, double* __restrict__ status,
                                       unsigned long long* __restrict__ counts) {
   if (threadIdx.x != 0) return;
-  double s = 0.0, sr = 0.0;
-  for (int i = 0; i < nparts; i++) { s += part[2 * i]; sr += part[2 * i + 1]; }
-  const double mean = s * inv_n_delta, meanr = sr * inv_n_delta;
-  int use = (mean >= 0.0) ? 1 : 0;  // NaN -> fallback
-  if (guard > 0.0 && !(meanr > 0.0 && mean <= guard * meanr && guard * mean >= meanr)) use = 0;
+  double sr = 0.0, sa = 0.0, sf = 0.0;
+  for (int i = 0; i < nparts; i++) { sr += part[3 * i]; sa += part[3 * i + 1]; sf += part[3 * i + 2]; }
+  const double raw = sr * inv_n_delta, applied = sa * inv_n_delta, ref = sf * inv_n_delta;
+  int use = (raw >= 0.0) ? 1 : 0;  // NaN -> fallback
+  if (guard > 0.0 && !(ref > 0.0 && applied <= guard * ref && guard * applied >= ref)) use = 0;
   flag[0] = use;
-  status[0] = mean;
+  status[0] = applied;
   status[1] = (double)use;
-  status[2] = meanr;
+  status[2] = ref;
+  status[3] = raw;
   counts[0] += 1ull;
   counts[1] += (unsigned long long)use;
 }

@@ -119,13 +119,13 @@ __device__ __forceinline__ void issue_layer(uint32_t d, uint32_t a_s, uint32_t w
 // 0..10 normalised inputs; 11..15 are multiplied by the zero-padded columns
 // of W1, so they may carry data for the epilogue).  out(p, valid, y, f0, f1,
 // P) consumes the 16 output columns (y[0..5] normalised outputs + biases)
-// and returns two terms summed per CTA into dissip_part[2 blockIdx.x] and
-// dissip_part[2 blockIdx.x + 1] (when non-null).
+// and returns three terms summed per CTA into dissip_part[3 blockIdx.x + j],
+// j = 0, 1, 2 (when non-null).
 // ------------------------------------------------------------------------
 constexpr int kInferGroups = 4;
 constexpr int kInferCtasPerSm = 2;  // 2 x 256 tensor-memory columns, 2 x 87 KB shared memory
-// after the activation tiles: G mbarriers, the tensor-memory slot and two
-// doubles per warp for the per-CTA sums (40 + 256 bytes at 16 warps)
+// after the activation tiles: G mbarriers, the tensor-memory slot and three
+// doubles per warp for the per-CTA sums (40 + 384 bytes at 16 warps)
 constexpr size_t kInferSmem = sizeof(MlpDev) + (size_t)kInferGroups * 16384 + 512;
 
 // One group's view of its tile: shared-memory addresses of its activation
@@ -251,7 +251,7 @@ k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long
   tc::fence_after_sync();
   const uint32_t tbase = *tslot;
   MlpGroup grp = mlp_group(P, act_all + (size_t)g * 16384, tbase, g, q, &bars[g]);
-  double dsum = 0.0, dsum2 = 0.0;
+  double dsum = 0.0, dsum2 = 0.0, dsum3 = 0.0;
   const long long ntiles = (n + 127) / 128;
   for (long long tile = (long long)blockIdx.x * G + g; tile < ntiles; tile += (long long)gridDim.x * G) {
     const long long p = tile * 128 + r;
@@ -263,23 +263,26 @@ k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long
       mlp_tile_failed(grp, r, err);
       break;
     }
-    const double2 d = out(p, valid, y, f0, f1, P);
+    const double3 d = out(p, valid, y, f0, f1, P);
     dsum += d.x;
     dsum2 += d.y;
+    dsum3 += d.z;
   }
   // per-CTA sums, fixed order
   for (int o = 16; o > 0; o >>= 1) {
     dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
     dsum2 += __shfl_xor_sync(0xffffffffu, dsum2, o);
+    dsum3 += __shfl_xor_sync(0xffffffffu, dsum3, o);
   }
-  if ((tid & 31) == 0) { red[2 * warp] = dsum; red[2 * warp + 1] = dsum2; }
+  if ((tid & 31) == 0) { red[3 * warp] = dsum; red[3 * warp + 1] = dsum2; red[3 * warp + 2] = dsum3; }
   tc::fence_before_sync();
   __syncthreads();
   if (tid == 0 && dissip_part) {
-    double s = 0.0, s2 = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { s += red[2 * w]; s2 += red[2 * w + 1]; }
-    dissip_part[2 * blockIdx.x] = s;
-    dissip_part[2 * blockIdx.x + 1] = s2;
+    double s = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { s += red[3 * w]; s2 += red[3 * w + 1]; s3 += red[3 * w + 2]; }
+    dissip_part[3 * blockIdx.x] = s;
+    dissip_part[3 * blockIdx.x + 1] = s2;
+    dissip_part[3 * blockIdx.x + 2] = s3;
   }
   if (warp == 0) {
     tc::fence_after_sync();
@@ -291,13 +294,13 @@ k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long
 // as f32 [n][8] (columns 6, 7 zero).
 struct MlpOutRaw {
   float* y;
-  __device__ double2 operator()(long long p, bool valid, const float (&v)[16], uint4, uint4, const MlpDev*) const {
+  __device__ double3 operator()(long long p, bool valid, const float (&v)[16], uint4, uint4, const MlpDev*) const {
     if (valid) {
       float4* o = reinterpret_cast<float4*>(y + 8 * p);
       o[0] = make_float4(v[0], v[1], v[2], v[3]);
       o[1] = make_float4(v[4], v[5], 0.f, 0.f);
     }
-    return make_double2(0.0, 0.0);
+    return make_double3(0.0, 0.0, 0.0);
   }
 };
 

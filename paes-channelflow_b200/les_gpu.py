@@ -297,8 +297,8 @@ class LesGpu:
         return used.value, d.value
 
     def set_learned_guard(self, ratio):
-        """Factor of the fallback test against the reference (Smagorinsky)
-        dissipation (default 4; <= 0 keeps only the sign test)."""
+        """Factor of the fallback test against the reference (Smagorinsky-Lilly,
+        C_s = 0.17) dissipation (default 4; <= 0 keeps only the sign test)."""
         self._check(lib().les_gpu_set_learned_guard(self.h, float(ratio)))
 
     def learned_reference(self):

@@ -36,8 +36,10 @@ widths, which is what carries it from the training grids to others.
    component correlation and normalised MSE of the deviatoric stresses for
    the network, for the Deardorff eddy viscosity -2 (0.1 Delta sqrt(e)) S
    with the filtered e = tau_kk / 2, and for Smagorinsky -2 (0.1 Delta)^2
-   |S| S; mean dissipations of the network, the filtered truth and the
-   Smagorinsky estimate the runtime fallback test compares with.
+   |S| S; the network as the solver applies it (local backscatter removed
+   along S) and raw; mean dissipations of the network, the filtered truth
+   and the Smagorinsky estimate (Lilly's C_s = 0.17) the runtime fallback
+   test compares with.
 6. Writes <out>.npz (params, norm, grids) and <out>.json (report).
 """
 import argparse
@@ -293,12 +295,16 @@ def apriori(mlp, feats, tau, norm, clip, delta):
     y = mlp.forward(x)[:, :6].double()
     n = torch.from_numpy(norm.astype(np.float64)).to(y.device)
     s = feats[:, 11].double()
-    tau_net = (y * n[22:28] + n[28:34]) * (s * s)[:, None]
+    tau_raw = (y * n[22:28] + n[28:34]) * (s * s)[:, None]
     t = tau.double()
     g = feats[:, :9].double() * (s / delta)[:, None]  # (ux, vx, wx, uy, vy, wy, uz, vz, wz)
     S = torch.stack([g[:, 0], g[:, 4], g[:, 8], 0.5 * (g[:, 3] + g[:, 1]), 0.5 * (g[:, 6] + g[:, 2]),
                      0.5 * (g[:, 7] + g[:, 5])], dim=1)
     w = torch.tensor([1.0, 1.0, 1.0, 2.0, 2.0, 2.0], dtype=torch.float64, device=S.device)
+    # the stress the solver applies: local backscatter (tau:S > 0) removed along S
+    ts, ss = (tau_raw * S * w).sum(1), (S * S * w).sum(1)
+    a = torch.where((ts > 0) & (ss > 0), -ts / torch.where(ss > 0, ss, torch.ones_like(ss)), torch.zeros_like(ts))
+    tau_net = tau_raw + a[:, None] * S
     smag = torch.sqrt(2.0 * (S * S * w).sum(1))
     e = torch.clamp(0.5 * (t[:, 0] + t[:, 1] + t[:, 2]), min=0.0)
     tau_dd = -2.0 * (0.1 * delta * torch.sqrt(e))[:, None] * S
@@ -309,15 +315,15 @@ def apriori(mlp, feats, tau, norm, clip, delta):
         a = td[:, i]
         var = float(((a - a.mean()) ** 2).mean())
         r = {}
-        for lab, p in (("network", deviatoric(tau_net)[:, i]), ("deardorff", deviatoric(tau_dd)[:, i]),
-                       ("smagorinsky", deviatoric(tau_sm)[:, i])):
+        for lab, p in (("network", deviatoric(tau_net)[:, i]), ("network_raw", deviatoric(tau_raw)[:, i]),
+                       ("deardorff", deviatoric(tau_dd)[:, i]), ("smagorinsky", deviatoric(tau_sm)[:, i])):
             rho = float(torch.corrcoef(torch.stack([a, p]))[0, 1])
             mse = float(((p - a) ** 2).mean()) / max(var, 1e-300)
             r[lab] = dict(rho=rho, nmse=mse)
         rep[nm] = r
     dis = lambda tt: float((-(tt * S * w).sum(1)).mean())
-    rep["dissipation"] = dict(network=dis(tau_net), filtered=dis(t), deardorff=dis(tau_dd),
-                              smagorinsky_reference=float((0.01 * delta ** 2 * smag ** 3).mean()))
+    rep["dissipation"] = dict(network=dis(tau_net), network_raw=dis(tau_raw), filtered=dis(t), deardorff=dis(tau_dd),
+                              smagorinsky_reference=float((0.17 ** 2 * delta ** 2 * smag ** 3).mean()))
     rep["dissipation"]["network_over_reference"] = rep["dissipation"]["network"] / rep["dissipation"][
         "smagorinsky_reference"]
     return rep

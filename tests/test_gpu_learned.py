@@ -91,7 +91,7 @@ def test_anti_dissipative_network_reproduces_deardorff(gpu_lib, product):
     o, g, m, f = learned_pair(product, sign)
     g.stage(0, True, 1)
     used, dis = g.learned_status()
-    assert used == 0 and dis < 0
+    assert used == 0 and dis >= 0  # rejected on the raw sign; the applied stress is projected
     _, d, _ = make_pair(product, 32, 32, 16, imodel=3, re_tau=RE_TAU)
     d.stage(0, True, 1)
     a, b = g.download(), d.download()

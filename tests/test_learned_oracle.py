@@ -31,14 +31,16 @@ def np_learned(cfg, fl, P, N):
     u, v, w = fl["u"], fl["v"], fl["w"]
     f, sc = LN.features(u, v, w, cfg.xl, cfg.yl, cfg.zl)
     y = LN.mlp(P, (f - N[:11]) * N[11:22])
-    tau = ((y * N[22:28] + N[28:34]) * (sc ** 2)[:, None]).T.reshape(6, NZ, NY, NX)
+    raw = ((y * N[22:28] + N[28:34]) * (sc ** 2)[:, None]).T.reshape(6, NZ, NY, NX)
     g = LN.gradients(u, v, w, cfg.xl, cfg.yl, cfg.zl)
+    tau = LN.project_backscatter(g, raw)
     dz = cfg.zl / NZ
     xkmax = dz * dz / cfg.dt / 5.0
     nut = LN.network_viscosity(g, tau, xkmax)
     dsl = (cfg.xl / NX * cfg.yl / NY * dz) ** (1.0 / 3.0)
     dis_r = LN.reference_dissipation(g, dsl)
-    return LN.dissipation(g, tau), dis_r, LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl, u, v, nut)
+    return (LN.dissipation(g, raw), LN.dissipation(g, tau), dis_r,
+            LN.divergence(tau, cfg.xl, cfg.yl, cfg.zl, u, v, nut))
 
 
 @pytest.mark.parametrize("guard", [0.0, 4.0, 1e6])
@@ -49,10 +51,12 @@ def test_learned_prepare_matches_numpy(sign, guard):
     o.set_learned_guard(guard)
     o.stage(0, 0, 1)
     used, dis = o.learned_status()
-    dis_np, dis_r_np, (lru, lrv, lrw) = np_learned(cfg, fl, P, N)
+    raw_np, dis_np, dis_r_np, (lru, lrv, lrw) = np_learned(cfg, fl, P, N)
     assert abs(dis - dis_np) <= 1e-9 * abs(dis_np)
+    assert abs(o.learned_raw() - raw_np) <= 1e-9 * abs(raw_np)
     assert abs(o.learned_reference() - dis_r_np) <= 1e-9 * abs(dis_r_np) and dis_r_np > 0
-    assert used == LN.network_used(dis_np, dis_r_np, guard)
+    assert dis_np >= max(raw_np, 0.0) - 1e-12 * abs(raw_np)  # the projection only removes backscatter
+    assert used == LN.network_used(raw_np, dis_np, dis_r_np, guard)
     if used:
         a, b, c = o.learned_divergence()
         for x, y in ((a, lru), (b, lrv), (c, lrw)):
@@ -69,7 +73,7 @@ def test_anti_dissipative_network_falls_back_to_deardorff():
         used, dis = o.learned_status()
         if used:
             continue
-        assert dis < 0
+        assert o.learned_raw() < 0 and dis >= 0  # the applied (projected) stress never injects energy
         cfg3 = O.make_config(NX, NY, NZ, re_tau=RE_TAU, imodel=3)
         d = O.Oracle(cfg3)
         d.set_fields(**fields)
