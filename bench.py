@@ -370,7 +370,8 @@ def main():
                 "config": {"workload": "channel 512x512x256 Re_tau=590 Deardorff isurface=6, sampled as a 512x512x4 slab",
                            "global_batch": NX * NY * SLAB_NZ, "parallelism": "cpu-openmp"},
                 "cpu_baseline": {"value": val, "unit": "Mpoint-steps/s", "cores": cores, "kind": "port",
-                                 "sample": "512x512x4 slab of the 512x512x256 grid, 1 RK3 step per timed step, FP64 oracle"},
+                                 "sample": "512x512x4 slab of the 512x512x256 grid, %d warm-up + %d timed RK3 steps, "
+                                           "FP64 oracle" % (args.warmup, args.steps)},
                 "e2e": {"value": val, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
