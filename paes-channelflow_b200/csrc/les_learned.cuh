@@ -241,24 +241,26 @@ template <class T> struct MlpOutTau {
     float g[9];
 #pragma unroll
     for (int j = 0; j < 9; j++) g[j] = (q[j] * P->in_rscale[j] + P->in_shift[j]) * s;  // d_i u_j * Delta
+    // per-point arithmetic in f32 (the network's own precision is bf16); the
+    // sums over the points are accumulated in f64 by the caller
     const float sv[6] = {g[0], g[4], g[8], 0.5f * (g[3] + g[1]), 0.5f * (g[6] + g[2]), 0.5f * (g[7] + g[5])};
-    const double ss = (double)sv[0] * sv[0] + (double)sv[1] * sv[1] + (double)sv[2] * sv[2] +
-                      2.0 * ((double)sv[3] * sv[3] + (double)sv[4] * sv[4] + (double)sv[5] * sv[5]);  // S:S
-    const double ts = (double)t[0] * sv[0] + (double)t[1] * sv[1] + (double)t[2] * sv[2] +
-                      2.0 * ((double)t[3] * sv[3] + (double)t[4] * sv[4] + (double)t[5] * sv[5]);  // tau:S
-    double applied = -ts;
-    if (ts > 0.0 && ss > 0.0) {
-      const float a = (float)(-ts / ss);
+    const float ss = sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2] +
+                     2.0f * (sv[3] * sv[3] + sv[4] * sv[4] + sv[5] * sv[5]);  // S:S
+    const float ts = t[0] * sv[0] + t[1] * sv[1] + t[2] * sv[2] +
+                     2.0f * (t[3] * sv[3] + t[4] * sv[4] + t[5] * sv[5]);  // tau:S
+    float applied = -ts;
+    if (ts > 0.0f && ss > 0.0f) {
+      const float a = -ts / ss;
 #pragma unroll
       for (int i = 0; i < 6; i++) t[i] += a * sv[i];
-      applied = 0.0;
+      applied = 0.0f;
     }
 #pragma unroll
     for (int i = 0; i < 6; i++) tau[(size_t)i * N + p] = (T)t[i];
     tau[(size_t)6 * N + p] = (T)(t[4] * g[6] + t[5] * g[7]);
     tau[(size_t)7 * N + p] = (T)(g[6] * g[6] + g[7] * g[7]);
-    const double sm2 = 2.0 * ss;  // (|S| Delta)^2
-    return make_double3(-ts, applied, kRefCs2 * sm2 * sqrt(sm2));
+    const float sm2 = 2.0f * ss;  // (|S| Delta)^2
+    return make_double3((double)-ts, (double)applied, kRefCs2 * (double)(sm2 * sqrtf(sm2)));
   }
 };
 
