@@ -14,6 +14,9 @@ Forms (each against the FP64 Deardorff run):
                      library's default fallback test (sign, and a factor 4
                      of the Smagorinsky estimate);
   learned_sign_only  the same with the sign test only.
+With --ref-production the FP64 reference and the mixed form add the TKE
+shear production the shipped Deardorff model lacks (a physically complete
+Deardorff LES); the learned forms keep the shipped TKE equation.
 At every checkpoint: the largest |U - U_fp64| over U_b, the largest <u'w'>
 and u_rms differences over their FP64 maxima, the largest relative
 difference of the u x-spectra (spectra2.f90:24-32) over the resolved band
@@ -42,11 +45,12 @@ def spec_levels(nz, re_tau, zl=2.0):
     return sorted({max(1, int(round(zp / (zl / nz * re_tau) + 0.5))) for zp in (15.0, 100.0)})
 
 
-def run(P, grid, re_tau, precision, imodel, steps, every, dt=None, mlp=None, guard=None, log=print):
+def run(P, grid, re_tau, precision, imodel, steps, every, dt=None, mlp=None, guard=None, log=print, production=0):
     """Checkpoints of one form: {step: (U, <u'w'>, u_rms, {level: u x-spectrum})}
     and the learned closure's (stages, used) counters per checkpoint."""
     nx, ny, nz = grid
-    cfg = P.channel_config(nx, ny, nz, dt=1e-3, re_tau=re_tau, precision=precision, imodel=imodel)
+    cfg = P.channel_config(nx, ny, nz, dt=1e-3, re_tau=re_tau, precision=precision, imodel=imodel,
+                           tke_production=production)
     g = P.LesGpu(cfg)
     if mlp is not None:
         g.set_mlp(mlp, re_tau)
@@ -123,6 +127,10 @@ def main(argv=None):
                     help="comma list of mixed, learned, learned_sign_only, learned_guard<factor>")
     ap.add_argument("--weights", default=os.path.join(HERE, "weights", "sgs_c4.npz"))
     ap.add_argument("--out", default="aposteriori.json")
+    ap.add_argument("--ref-production", action="store_true",
+                    help="the FP64 Deardorff reference (and the mixed form) with the TKE shear production "
+                         "term the shipped model lacks (tke_production = 1); the learned forms keep the "
+                         "shipped TKE equation")
     a = ap.parse_args(argv)
     P = load()
     forms = a.forms.split(",")
@@ -131,15 +139,18 @@ def main(argv=None):
         z = np.load(a.weights)
         mlp = P.Mlp(z["params"], z["norm"])
     print("fp64 Deardorff")
-    ref, _, dt = run(P, a.grid, a.re_tau, P.PREC_FP64, P.SGS_DEARDORFF, a.steps, a.every)
+    ref, _, dt = run(P, a.grid, a.re_tau, P.PREC_FP64, P.SGS_DEARDORFF, a.steps, a.every,
+                     production=int(a.ref_production))
     res = {"grid": a.grid, "re_tau": a.re_tau, "dt": dt, "steps": a.steps, "every": a.every,
+           "reference_tke_production": int(a.ref_production),
            "spectrum_levels": spec_levels(a.grid[2], a.re_tau), "weights": os.path.basename(a.weights),
            "forms": {}}
     for name in forms:
         print(name)
         try:
             if name == "mixed":
-                r = run(P, a.grid, a.re_tau, P.PREC_MIXED, P.SGS_DEARDORFF, a.steps, a.every, dt)
+                r = run(P, a.grid, a.re_tau, P.PREC_MIXED, P.SGS_DEARDORFF, a.steps, a.every, dt,
+                        production=int(a.ref_production))
             elif name == "learned":
                 r = run(P, a.grid, a.re_tau, P.PREC_MIXED, P.SGS_LEARNED, a.steps, a.every, dt, mlp)
             elif name == "learned_sign_only":
