@@ -57,16 +57,24 @@ int main(int argc, char** argv) {
   c.imodel = LES_SGS_DEARDORFF; c.isurface = 6; c.precision = LES_PREC_FP64;
   c.xl = 2.0 * M_PI; c.yl = M_PI; c.zl = 2.0;
   c.z0 = std::exp(-0.4 * 5.0) * 1.0 / re_tau;
-  c.dt = 1e-3;  // replaced below by the CFL step; the stage calls take dtab1, dtab2 explicitly
-  les_handle* h = nullptr;
-  check(nullptr, les_gpu_init(&c, &h), "les_gpu_init");
-
-  // initial field (replaces initvel + deal)
   const double utau = std::sqrt(0.016);
   const double ub = utau * ((std::log(re_tau) - 1.0) / 0.4 + 5.0);
-  check(h, les_gpu_make_ic(h, 12345ull, ub, 0.1, utau, 1e-4), "les_gpu_make_ic");
+  // the namelist's fixed dt: CFL 0.5 of the initial field (les.F90:205-208),
+  // from a first handle holding that field
   double dt = 0.0;
-  check(h, les_gpu_cfl_dt(h, 0.5, &dt), "les_gpu_cfl_dt");
+  {
+    c.dt = 1e-3;
+    les_handle* t = nullptr;
+    check(nullptr, les_gpu_init(&c, &t), "les_gpu_init");
+    check(t, les_gpu_make_ic(t, 12345ull, ub, 0.1, utau, 1e-4), "les_gpu_make_ic");
+    check(t, les_gpu_cfl_dt(t, 0.5, &dt), "les_gpu_cfl_dt");
+    les_gpu_finalize(t);
+  }
+  c.dt = dt;
+  les_handle* h = nullptr;
+  check(nullptr, les_gpu_init(&c, &h), "les_gpu_init");
+  // initial field (replaces initvel + deal)
+  check(h, les_gpu_make_ic(h, 12345ull, ub, 0.1, utau, 1e-4), "les_gpu_make_ic");
   const double dz = c.zl / nnz;
 
   std::vector<double> meanbuf((size_t)19 * nnz), sc(5);

@@ -19,7 +19,7 @@ Tolerances grow with the step count because the two implementations sum in
 different orders and the flow amplifies round-off differences: FP64
 1e-9 after 10 steps, 1e-7 after 100; after 1000 steps of C2 the flow has
 left the laminar start and the fields are compared statistically (mean
-profile and moments) with the bounds below.
+profile, moments and sampled planes) with the bounds below.
 """
 import os
 import sys
@@ -38,9 +38,9 @@ pytestmark = pytest.mark.gpu
 # field-wise (planes, projections, RMS) and statistics tolerances per snapshot
 TOL_FIELD = {10: 1e-9, 100: 1e-7}
 TOL_STATS = {10: 1e-9, 100: 1e-7}
-# after 1000 steps (C2): the flow is no longer bitwise comparable; the mean
-# profile and the plane RMS values must still agree closely
-TOL_1000 = dict(mean_u=1e-3, rms=2e-2, moments=5e-2)
+# after 1000 steps (C2): round-off differences have grown (sampled planes agree to
+# ~1e-2 of their scale); the mean profile, plane RMS and moments still agree closely
+TOL_1000 = dict(mean_u=1e-4, rms=1e-3, moments=2e-2, plane=5e-2)
 
 
 def _rel(a, b):
@@ -85,7 +85,10 @@ def _run_case(product, case):
         mbo = fx["s%d_meanbuf" % n]
         r["mean_u"] = _rel(mb[3], mbo[3])
         r["moments"] = max(_rel(mb[i], mbo[i]) for i in (0, 6, 7, 8, 9, 11))
-        r["sgs"] = max(_rel(mb[i], mbo[i]) for i in (13, 14, 15, 16, 17))
+        # SGS means (uusb..vwsb): the interior rows are plane means of nu_t times a velocity
+        # gradient, near-cancelling sums; all six are held to the scale of the wall-stress rows
+        sgs_scale = max(np.abs(mbo[17]).max(), np.abs(mbo[18]).max())
+        r["sgs"] = max(float(np.abs(mb[i] - mbo[i]).max() / sgs_scale) for i in range(13, 19))
         r["scalars"] = _rel(sc[:2], fx["s%d_scalars" % n][:2])
         spec = np.array([G.xspectrum(f["u"][z]) for z in G.sample_levels(nz)])
         r["xspec_u"] = _rel(spec, fx["s%d_xspec_u" % n])
@@ -111,6 +114,7 @@ def _check(fx, report, div):
                 assert v < tol, (n, k, v, tol)
         else:
             assert r["mean_u"] < TOL_1000["mean_u"], (n, r)
+            assert max(r["plane_" + k] for k in "uvw") < TOL_1000["plane"], (n, r)
             assert max(r["rms_" + k] for k in "uvw") < TOL_1000["rms"], (n, r)
             assert r["moments"] < TOL_1000["moments"], (n, r)
 
