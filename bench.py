@@ -149,9 +149,11 @@ def bf16_peak_tflops():
         return 1400.0, "fallback sustained"
 
 
-def algorithmic_bytes(kernel, nx, ny, nz, tb):
+def algorithmic_bytes(kernel, nx, ny, nz, tb, learned=False):
     """Compulsory HBM bytes of one launch (one stage over all levels) of the
-    stage kernels: every array the kernel must read once and write once."""
+    stage kernels: every array the kernel must read once and write once.
+    With the learned closure the fused row kernel leaves the UY and WY
+    inputs unread (only ux and vy of the gradients are transformed)."""
     mx, my, kx = 3 * nx // 2, 3 * ny // 2, nx // 2
     pad = mx * my * tb            # padded physical plane
     mix = my * kx * 2 * tb        # x-spectral, y-physical plane on the padded y grid
@@ -172,7 +174,7 @@ def algorithmic_bytes(kernel, nx, ny, nz, tb):
         "k_press": nz * (9 * spec + 2 * 24 * nm + 16 * nm),
         "k_update": nz * (15 * spec + 16 * nm),
         # fused row kernel: reads the 8 mixed inputs, writes the 8 mixed outputs
-        "k_row_fused": 2 * (4 * L + 4 * Lw) * mix,
+        "k_row_fused": ((3 * L + 3 * Lw) if learned else (4 * L + 4 * Lw)) * mix + (4 * L + 4 * Lw) * mix,
     }
     return table.get(kernel)
 
@@ -438,7 +440,7 @@ def main():
     top = max(agg.items(), key=lambda kv: kv[1][1])
     kname, (kfull, kms) = top[0], top[1]
     peak, peak_kind = peaks()
-    ab = algorithmic_bytes(kname, NX, NY, NZ, 4)
+    ab = algorithmic_bytes(kname, NX, NY, NZ, 4, learned=True)
     achieved = ab / (kms / 1e3) / 1e9 if ab else None
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic_k_row_fused_512x512x256.txt")
@@ -449,15 +451,18 @@ def main():
                 traffic = float(f[2])
     stage_ms = sum(t for _, t in prof)
     # compute roof of the fused row kernel: its transform and pointwise flops
-    # (12 complex transforms of 3nx/2 points at 5 N log2 N, ~150 flops per
-    # point of the pointwise rows) per padded row and level, against the
+    # (12 complex transforms of 3nx/2 points at 5 N log2 N -- 10 with the
+    # learned closure, whose phase I skips UY+iVY and WX+iWY -- and ~150 flops
+    # per point of the pointwise rows) per padded row and level, against the
     # device's FP32 / FP64 FMA rate from the library's probe kernel
     mxp = 3 * NX // 2
-    row_flops = 3 * NY // 2 * NZ * (12 * 5.0 * mxp * np.log2(mxp) + 150.0 * mxp)
+    def fused_flops(transforms):
+        return 3 * NY // 2 * NZ * (transforms * 5.0 * mxp * np.log2(mxp) + 150.0 * mxp)
     fma32, fma64 = P.fma_rate(4, dev), P.fma_rate(8, dev)
-    def compute_roof(profile, peak):
+    def compute_roof(profile, peak, transforms=12):
+        row_flops = fused_flops(transforms)
         ms = sum(t for n, t in profile if n.startswith("k_row_fused"))
-        return {"kernel": "k_row_fused", "flops_per_launch": row_flops, "kernel_ms": ms,
+        return {"kernel": "k_row_fused", "transforms_per_row": transforms, "flops_per_launch": row_flops, "kernel_ms": ms,
                 "achieved_tflops": row_flops / (ms / 1e3) / 1e12, "peak_tflops": peak / 1e12,
                 "frac": row_flops / (ms / 1e3) / peak, "peak_source": "les_probe_fma_rate (measured FMA rate)"}
     # the network's tensor-core kernel: 2*(11*64 + 2*64*64 + 64*6) flops per point
@@ -502,7 +507,7 @@ def main():
         "roofline_network": {"bound": "tensor", "kernel": "k_mlp_infer", "achieved": mlp_tf, "peak": bf16_peak,
                              "unit": "TFLOP/s", "frac": (mlp_tf / bf16_peak) if mlp_tf else None,
                              "kernel_ms": mlp_ms, "flops_per_point": fpp, "peak_source": bf16_kind},
-        "roofline_compute": {"learned_mixed_f32": compute_roof(prof, fma32), "mixed_f32": compute_roof(prof32, fma32),
+        "roofline_compute": {"learned_mixed_f32": compute_roof(prof, fma32, transforms=10), "mixed_f32": compute_roof(prof32, fma32),
                              "fp64": compute_roof(prof64, fma64)},
         "kernels_ms_stage2_learned_mixed": {n: round(t, 4) for n, t in prof},
         "kernels_ms_stage2_fp64": {n: round(t, 4) for n, t in prof64},

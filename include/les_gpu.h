@@ -178,11 +178,17 @@ long long les_gpu_kernel_launches(les_handle* h);
 
 /* Tracing: run one stage (not graph-captured) with a CUDA event recorded
  * after every kernel on the handle's stream; ms[i] is the duration of the
- * i-th kernel and kernels[i] its host stub address (match it against
- * dladdr / the exported kernel symbols).  *nkernels receives the count; at
- * most cap entries are written.  Advances the state by one stage. */
+ * i-th kernel and kernels[i] its host stub address (les_gpu_kernel_name
+ * resolves it).  *nkernels receives the count; at most cap entries are
+ * written.  Advances the state by one stage. */
 int les_gpu_profile_stage(les_handle* h, int istage, double dt, double* ms,
                           const void** kernels, int cap, int* nkernels);
+
+/* The device-side (mangled) name of the kernel whose host stub address is
+ * `kernel` (as returned by les_gpu_profile_stage), NUL-terminated into
+ * buf[cap]; kernels of internal linkage included.  LES_EINVAL for a NULL
+ * argument or an address that is no kernel of this library. */
+int les_gpu_kernel_name(const void* kernel, char* buf, int cap);
 
 /* sizeof(les_config) as compiled into the library (binding sanity check). */
 size_t les_gpu_config_size(void);

@@ -417,6 +417,18 @@ int les_gpu_profile_stage(les_handle* h, int istage, double dt, double* ms, cons
   return rc;
 }
 
+int les_gpu_kernel_name(const void* kernel, char* buf, int cap) {
+  if (!kernel || !buf || cap < 1) return LES_EINVAL;
+  const char* name = nullptr;
+  if (cudaFuncGetName(&name, kernel) != cudaSuccess || !name) {
+    cudaGetLastError();
+    buf[0] = 0;
+    return LES_EINVAL;
+  }
+  snprintf(buf, (size_t)cap, "%s", name);
+  return LES_OK;
+}
+
 int les_op_xderiv(const void* ain, void* ax, int n1, int n2, int howmany, double xl, int real_bytes, void* stream) {
   if (!ain || !ax || n1 <= 0 || n2 <= 0 || howmany <= 0 || !(xl > 0) || check_rb(real_bytes)) return LES_EINVAL;
   return op_guard([&] {

@@ -113,6 +113,7 @@ def lib():
         "les_gpu_cfl_dt": (I, [H, D, ctypes.POINTER(D)]),
         "les_gpu_kernel_launches": (ctypes.c_longlong, [H]),
         "les_gpu_profile_stage": (I, [H, I, D, VP, VP, I, ctypes.POINTER(I)]),
+        "les_gpu_kernel_name": (I, [VP, ctypes.c_char_p, I]),
         "les_gpu_stream": (VP, [H]),
         "les_op_xderiv": (I, [VP, VP, I, I, I, D, I, VP]),
         "les_op_yderiv": (I, [VP, VP, I, I, I, D, I, VP]),
@@ -398,27 +399,21 @@ class LesGpu:
         return [(kernel_name(fn[i]), ms[i]) for i in range(min(n.value, cap))]
 
 
-class _DlInfo(ctypes.Structure):
-    _fields_ = [("dli_fname", ctypes.c_char_p), ("dli_fbase", ctypes.c_void_p),
-                ("dli_sname", ctypes.c_char_p), ("dli_saddr", ctypes.c_void_p)]
-
-
 def kernel_name(addr):
-    """Short name of a kernel from its host stub address (dladdr + a light
-    demangling of les::k_<name><T, N>)."""
-    libdl = ctypes.CDLL(None)
-    info = _DlInfo()
-    if not addr or not libdl.dladdr(ctypes.c_void_p(addr), ctypes.byref(info)) or not info.dli_sname:
-        return hex(addr or 0)
-    raw = info.dli_sname.decode()
+    """Short name of a kernel from its host stub address: the device name
+    (les_gpu_kernel_name) lightly demangled from les::k_<name><T, N>."""
     import re
-    m = re.match(r"_ZN3les(\d+)(k_\w+)", raw)
+    buf = ctypes.create_string_buffer(1024)
+    if not addr or lib().les_gpu_kernel_name(ctypes.c_void_p(addr), buf, len(buf)) != LES_OK:
+        return hex(addr or 0)
+    raw = buf.value.decode()
+    m = re.match(r"_ZN3les(?:12_GLOBAL__N_1)?L?(\d+)(k_\w+)", raw)
     if not m:
         return raw
     n = int(m.group(1))
     name = m.group(2)[:n]
     tail = raw[m.end(1) + n:]
-    tp = "f64" if tail.startswith("IdL") or tail.startswith("Id") else ("f32" if tail.startswith("If") else "")
+    tp = "f64" if tail.startswith("Id") else ("f32" if tail.startswith("If") else "")
     num = re.match(r"I[df]Li(\d+)", tail)
     return name + ("<%s%s>" % (tp, "," + num.group(1) if num else "") if tp else "")
 

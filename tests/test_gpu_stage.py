@@ -114,6 +114,18 @@ def test_graph_step_matches_stages(gpu_lib, product):
     assert g2.kernel_launches() > 0
 
 
+def test_profile_stage_names_every_kernel(gpu_lib, product):
+    """The per-kernel trace of one stage resolves every launch (internal
+    linkage kernels such as k_wall_final included) to its les:: kernel name."""
+    o, g, f = make_pair(product, 32, 32, 16)
+    prof = g.profile_stage(2)
+    names = [n for n, _ in prof]
+    assert len(names) > 5
+    assert all(n.startswith("k_") for n in names), names
+    assert "k_wall_final" in names and any(n.startswith("k_row_fused") for n in names), names
+    assert all(t >= 0 for _, t in prof)
+
+
 def test_c1_ten_steps_fp64(gpu_lib, product):
     """Config 1 (64^3, Re_tau 180, Deardorff, isurface 6): 10 RK3 steps."""
     cfg_o = O.make_config(64, 64, 64, dt=1e-3, re_tau=180.0)
