@@ -203,6 +203,10 @@ struct Engine : EngineBase {
   DevBuf<T> ephys, dEX, dEY, wallpl;
   DevBuf<cx<T>> xout[8];  // Xu1..Xe2 written by k_row_fused (its inputs stay readable)
   DevBuf<double> divacc, sgsacc, wacc, acc;
+  // per-(level, block) partial sums of divz and the SGS means, reduced into
+  // divacc / sgsacc in a fixed order when the statistics are read
+  DevBuf<double> divpart, sgspart;
+  int nstat_parts = 0;
   DevBuf<WallParams> wp;
   DevBuf<int> err;
   DevBuf<unsigned long long> amax;
@@ -265,6 +269,9 @@ struct Engine : EngineBase {
       for (auto& b : flux) b.alloc(pb * NZ);
     }
     divacc.alloc(NZ); sgsacc.alloc((size_t)NZ * 8); wacc.alloc((size_t)2 * kWallBlocks * 8); acc.alloc((size_t)NZ * 16);
+    // one partial per padded row (k_row_fused) or per 256-point block (k_flux)
+    nstat_parts = fused ? MY : (int)cdiv(pb, 256);
+    divpart.alloc((size_t)NZ * nstat_parts); sgspart.alloc((size_t)NZ * nstat_parts * 6);
     wp.alloc(1); err.alloc(1); amax.alloc(4);
     for (auto& b : phys) b.alloc(ps * (NZ + 2));
     stage_buf.alloc(ps * NZ * 8);
@@ -273,7 +280,7 @@ struct Engine : EngineBase {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
     for (auto* b : {&uh, &vh, &wh, &ruo, &rvo, &rwo, &run, &rvn, &rwn, &Xe, &rem}) b->release();
-    for (auto* b : {&mu, &mv, &mru, &mrv, &dscr, &divacc, &sgsacc, &wacc, &acc}) b->release();
+    for (auto* b : {&mu, &mv, &mru, &mrv, &dscr, &divacc, &sgsacc, &wacc, &acc, &divpart, &sgspart}) b->release();
     ph.release(); rscr.release(); e.release(); re.release(); wp.release(); err.release(); amax.release();
     stage_buf.release();
     for (auto& b : mixed) b.release();
@@ -450,8 +457,6 @@ struct Engine : EngineBase {
 
   // ---- the stage ----
   void comp1_kernels(const StageArgs& a) {
-    LES_CUDA(cudaMemsetAsync(divacc.p, 0, NZ * sizeof(double), st));
-    if (a.mnout_sgs) LES_CUDA(cudaMemsetAsync(sgsacc.p, 0, (size_t)NZ * 8 * sizeof(double), st));
     const T dtab2 = (T)a.dtab2;
     // the learned closure reads the stage's start state (u, v, w and, for
     // its fallback test, e before k_e_prep's zeta update)
@@ -764,7 +769,7 @@ struct Engine : EngineBase {
     FusedArgs fa{};
     for (int i = 0; i < 8; i++) { fa.in.p[i] = mixed[i].p; fa.out.p[i] = xout[i].p; }
     fa.dEX = dEX.p; fa.dEY = dEY.p; fa.clipflag = clipflag.p; fa.wp = wp.p;
-    fa.divacc = divacc.p; fa.sgsacc = sgsacc.p;
+    fa.divpart = divpart.p; fa.sgspart = sgspart.p;
     fa.lflag = learned_on() ? lflag.p : nullptr;
     int nch = (int)cdiv(8 * 148, MY);
     nch = std::max(1, std::min(nch, NZ / 8 > 0 ? NZ / 8 : 1));
@@ -809,8 +814,8 @@ struct Engine : EngineBase {
     }
     Ptr11 fl{};
     for (int i = 0; i < 11; i++) fl.p[i] = flux[i].p;
-    launch(k_flux<T>, dim3(cdiv(pb, 256), NZ), dim3(256), 0, st, pd, fl, a, (const WallParams*)wp.p, divacc.p,
-           sgsacc.p);
+    launch(k_flux<T>, dim3(cdiv(pb, 256), NZ), dim3(256), 0, st, pd, fl, a, (const WallParams*)wp.p, divpart.p,
+           sgspart.p);
     Ptr8 X{};
     for (int i = 0; i < 8; i++) X.p[i] = mixed[i].p;  // reuse the mixed buffers
     with_small(NX, [&](auto cn) {
@@ -956,9 +961,10 @@ struct Engine : EngineBase {
     to_physical(vh.p, phys[1].p, NZ);
     to_physical(wh.p, phys[2].p, NZ);
     LES_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)NZ * 16 * sizeof(double), st));
-    unsigned nb = std::min<unsigned>(cdiv(ps, 256), 256);
-    launch(k_plane_sums<T>, dim3(nb, NZ), dim3(256), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
+    launch(k_plane_sums<T>, dim3(1, NZ), dim3(1024), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
            (const T*)phys[2].p, (const T*)(e.p + ps), ps, acc.p);
+    launch(k_sum_parts, dim3(NZ), dim3(256), 0, st, (const double*)divpart.p, nstat_parts, 1, divacc.p, 1);
+    launch(k_sum_parts, dim3(NZ), dim3(256), 0, st, (const double*)sgspart.p, nstat_parts, 6, sgsacc.p, 8);
     std::vector<double> sums((size_t)NZ * 16), mshadow(NZ), vshadow(NZ);
     LES_CUDA(cudaMemcpyAsync(sums.data(), acc.p, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     LES_CUDA(cudaMemcpyAsync(mshadow.data(), mu.p, NZ * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -972,7 +978,7 @@ struct Engine : EngineBase {
     LES_CUDA(cudaMemcpyAsync(acc.p + (size_t)NZ * 8, means.data(), means.size() * sizeof(double),
                              cudaMemcpyHostToDevice, st));
     LES_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)NZ * 8 * sizeof(double), st));
-    launch(k_moments<T>, dim3(nb, NZ), dim3(256), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
+    launch(k_moments<T>, dim3(1, NZ), dim3(1024), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
            (const T*)phys[2].p, ps, NZ, (const double*)(acc.p + (size_t)NZ * 8), acc.p);
     std::vector<double> mom((size_t)NZ * 8), dv(NZ), sg((size_t)NZ * 8);
     WallParams w;
@@ -1088,8 +1094,7 @@ struct Engine : EngineBase {
     to_spectral(phys[2].p, wh.p, NZ);
     // FP64 plane means of the mean profile
     LES_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)NZ * 16 * sizeof(double), st));
-    unsigned nb = std::min<unsigned>(cdiv(ps, 256), 256);
-    launch(k_plane_sums<T>, dim3(nb, NZ), dim3(256), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
+    launch(k_plane_sums<T>, dim3(1, NZ), dim3(1024), 0, st, (const T*)phys[0].p, (const T*)phys[1].p,
            (const T*)nullptr, (const T*)nullptr, ps, acc.p);
     std::vector<double> s((size_t)NZ * 16);
     LES_CUDA(cudaMemcpyAsync(s.data(), acc.p, s.size() * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -196,8 +196,8 @@ struct FusedArgs {
   const void* dEY;
   const int* clipflag;   // per level 1..nnz-1 (index z-1)
   const WallParams* wp;
-  double* divacc;
-  double* sgsacc;
+  double* divpart;  // [level][y] partial sums of divz, one writer each
+  double* sgspart;  // [level][y][6] partial SGS means (stage 1 with mnout)
   // learned closure: when lflag is set and *lflag != 0 the interior momentum
   // stresses are left to the network (the wall-model rows stay)
   const int* lflag;
@@ -458,12 +458,13 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
     __syncthreads();
     // per-level statistics of this row
     {
+      const size_t slot = (size_t)(z - 1) * MY + y;
       double v1[1] = {divz_part};
-      block_sum_atomic<1>(v1, f.divacc + (z - 1));
+      block_sum_store<1>(v1, f.divpart + slot);
       divz_part = 0.0;
       if (a.mnout_sgs) {
         __syncthreads();
-        block_sum_atomic<6>(sgs_part, f.sgsacc + (size_t)(z - 1) * 8);
+        block_sum_store<6>(sgs_part, f.sgspart + slot * 6);
 #pragma unroll
         for (int q = 0; q < 6; q++) sgs_part[q] = 0.0;
       }

@@ -77,29 +77,6 @@ constexpr int ERR_NAN = 1, ERR_UTAU = 2;
 template <class T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
 template <class T> __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
 
-// Block-wide sum of `n` doubles per thread into acc[] with atomics.
-template <int NV>
-__device__ __forceinline__ void block_sum_atomic(double (&v)[NV], double* acc) {
-  __shared__ double red[32][NV];
-#pragma unroll
-  for (int q = 0; q < NV; q++)
-    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0)
-#pragma unroll
-    for (int q = 0; q < NV; q++) red[warp][q] = v[q];
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int q = 0; q < NV; q++) {
-      double s = (lane < nw) ? red[lane][q] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) atomicAdd(acc + q, s);
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Generic small-grid transforms (upload, download, deal, expand, compress)
 // ---------------------------------------------------------------------------
@@ -478,6 +455,23 @@ __device__ __forceinline__ void block_sum_store(double (&v)[NV], double* out) {
   }
 }
 
+// Per-level totals of per-block partial sums: one block per level z,
+// out[z*ostride + q] = sum over p < nparts of part[(z*nparts + p)*nq + q],
+// q < nq <= 8, summed in a fixed order.
+static __global__ void __launch_bounds__(256) k_sum_parts(const double* __restrict__ part, int nparts, int nq,
+                                                          double* __restrict__ out, int ostride) {
+  const size_t z = blockIdx.x;
+  double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int p = threadIdx.x; p < nparts; p += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+      if (q < nq) s[q] += part[(z * nparts + p) * nq + q];
+  double t[8];
+  block_sum_store<8>(s, t);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < nq; q++) out[z * ostride + q] = t[q];
+}
+
 // Raw sums over the padded planes U, V at level 1 (blockIdx.y = 0) and nnz
 // (blockIdx.y = 1): sum U, V, wind, U^2, V^2, wind^2, wind*U, wind*V, one
 // partial per block in part[side][block][8] (summed in order by k_wall_final).
@@ -601,8 +595,8 @@ __device__ __forceinline__ void wall_stress(const WallSide& w, const WallParams&
 struct Ptr11 { void* p[11]; };
 template <class T>
 __global__ void __launch_bounds__(256)
-k_flux(Ptr12 in, Ptr11 out, StageArgs a, const WallParams* __restrict__ wpp, double* __restrict__ divacc,
-       double* __restrict__ sgsacc) {
+k_flux(Ptr12 in, Ptr11 out, StageArgs a, const WallParams* __restrict__ wpp, double* __restrict__ divpart,
+       double* __restrict__ sgspart) {
   const int z = blockIdx.y + 1;
   const int NZ = a.NZ;
   const size_t P = (size_t)a.MX * a.MY;
@@ -693,11 +687,13 @@ k_flux(Ptr12 in, Ptr11 out, StageArgs a, const WallParams* __restrict__ wpp, dou
       *o[4] = (T)0;  // G at the top level (pairs with C in the forward transform)
     }
   }
-  // statistics: divz (every stage) and the SGS means (stage 1 with mnout)
+  // statistics: divz (every stage) and the SGS means (stage 1 with mnout),
+  // one partial sum per (level, block)
+  const size_t slot = (size_t)(z - 1) * gridDim.x + blockIdx.x;
   {
     T d = ux + vy + wz0;
     double s1[1] = {valid ? (double)(d * d) : 0.0};
-    block_sum_atomic<1>(s1, divacc + (z - 1));
+    block_sum_store<1>(s1, divpart + slot);
   }
   if (a.mnout_sgs) {
     __syncthreads();
@@ -708,7 +704,7 @@ k_flux(Ptr12 in, Ptr11 out, StageArgs a, const WallParams* __restrict__ wpp, dou
     st[3] = valid ? (double)tww0 : 0.0;
     st[4] = valid ? (double)tuw0 : 0.0;
     st[5] = valid ? (double)tvw0 : 0.0;
-    block_sum_atomic<6>(st, sgsacc + (size_t)(z - 1) * 8);
+    block_sum_store<6>(st, sgspart + slot * 6);
   }
 }
 
@@ -1043,8 +1039,9 @@ __global__ void k_ic_fill(T* __restrict__ out, int f, unsigned long long seed, i
 }
 
 // Per-level plane sums (FP64) of up to 4 small-grid fields: acc[z*8 + q].
+// One block per level (blockIdx.y), so the sums are reproducible.
 template <class T>
-__global__ void k_plane_sums(const T* __restrict__ f0, const T* __restrict__ f1, const T* __restrict__ f2,
+__global__ void __launch_bounds__(1024) k_plane_sums(const T* __restrict__ f0, const T* __restrict__ f1, const T* __restrict__ f2,
                              const T* __restrict__ f3, size_t P, double* acc) {
   const size_t off = (size_t)blockIdx.y * P;
   double s[4] = {0, 0, 0, 0};
@@ -1054,14 +1051,15 @@ __global__ void k_plane_sums(const T* __restrict__ f0, const T* __restrict__ f1,
     if (f2) s[2] += (double)f2[off + i];
     if (f3) s[3] += (double)f3[off + i];
   }
-  block_sum_atomic<4>(s, acc + (size_t)blockIdx.y * 8);
+  block_sum_store<4>(s, acc + (size_t)blockIdx.y * 8);
 }
 
 // Moments of compmn (compmn.F90:29-62) at level iz = blockIdx.y + 1:
 // u, v, w are small-grid physical fields on levels 1..nnz (u, v at nnz+1 are
-// zero); means[z*8 + 0/1] hold the plane means of u and v.
+// zero); means[z*8 + 0/1] hold the plane means of u and v.  One block per
+// level, as k_plane_sums.
 template <class T>
-__global__ void k_moments(const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, size_t P, int NZ,
+__global__ void __launch_bounds__(1024) k_moments(const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w, size_t P, int NZ,
                           const double* __restrict__ means, double* acc) {
   const int iz = blockIdx.y + 1;
   const size_t off = (size_t)(iz - 1) * P;
@@ -1078,7 +1076,7 @@ __global__ void k_moments(const T* __restrict__ u, const T* __restrict__ v, cons
     s[0] += (double)(ul * ul); s[1] += (double)(vl * vl); s[2] += (double)(w0 * w0);
     s[3] += (double)(ul * w0); s[4] += (double)(vl * w0); s[5] += (double)(ul * vl);
   }
-  block_sum_atomic<6>(s, acc + (size_t)(iz - 1) * 8);
+  block_sum_store<6>(s, acc + (size_t)(iz - 1) * 8);
 }
 
 // Max |u|, |v|, |w| for the CFL time step (les.F90:205-207).

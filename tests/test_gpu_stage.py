@@ -114,6 +114,29 @@ def test_graph_step_matches_stages(gpu_lib, product):
     assert g2.kernel_launches() > 0
 
 
+@pytest.mark.parametrize("imodel,tke", [(3, 0), (3, 1)])
+def test_initial_field_and_statistics_are_reproducible(gpu_lib, product, imodel, tke):
+    """make_ic's plane means and compmn's divz / SGS-mean rows are per-block
+    partial sums reduced in a fixed order: two handles stepping the same
+    field agree bit for bit (fused row kernel and, with TKE production, the
+    unfused k_flux path)."""
+    out = []
+    for _ in range(2):
+        cfg = product.channel_config(32, 32, 16, dt=2e-3, re_tau=180.0, imodel=imodel, tke_production=tke)
+        g = product.LesGpu(cfg)
+        g.make_ic(seed=5, amp=0.2, re_tau=180.0)
+        for it in range(3):
+            g.step(it=it, mnout=True)
+        g.sync()
+        out.append((g.download(), g.stats()))
+        g.close()
+    (fa, (ma, sa)), (fb, (mb, sb)) = out
+    for k in "uvwep":
+        assert np.array_equal(fa[k], fb[k]), k
+    assert np.array_equal(ma, mb) and np.array_equal(sa, sb)
+    assert np.abs(ma[13:19]).max() > 0 and ma[2].max() > 0
+
+
 def test_profile_stage_names_every_kernel(gpu_lib, product):
     """The per-kernel trace of one stage resolves every launch (internal
     linkage kernels such as k_wall_final included) to its les:: kernel name."""
