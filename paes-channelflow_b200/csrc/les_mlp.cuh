@@ -102,6 +102,31 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* __r
   }
 }
 
+// Inference epilogue: 2 GELU(z) = z + z tanh(u) of the 64 accumulator
+// columns (the biases are already in the accumulators), written as row r of
+// a K = 64 activation tile.  The factor 2 is taken back by the halved
+// weights of the next layer (infer_prologue); both scalings are exact in
+// bf16, so the next layer's products equal those of GELU(z) and W.
+__device__ __forceinline__ uint32_t gelu2_pack(float a, float b) {
+  const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
+  const __nv_bfloat162 c = __floats2bfloat162_rn(kGeluC, kGeluC);
+  const __nv_bfloat162 ca = __floats2bfloat162_rn(kGeluC * kGeluA, kGeluC * kGeluA);
+  const __nv_bfloat162 u = __hmul2(x, __hfma2(__hmul2(x, x), ca, c));
+  return tc::bf2_bits(__hfma2(x, tc::tanh_bf2(u), x));
+}
+__device__ __forceinline__ void hidden_epilogue_infer(uint32_t taddr, unsigned char* act, int r) {
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    float v[16];
+    tc::tmem_ld16(taddr + 16 * c, v);
+    uint32_t pk[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) pk[j] = gelu2_pack(v[2 * j], v[2 * j + 1]);
+    *reinterpret_cast<uint4*>(act + 2 * tc::tile_elem(r, 16 * c, 64)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    *reinterpret_cast<uint4*>(act + 2 * tc::tile_elem(r, 16 * c + 8, 64)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+  }
+}
+
 // MMA issue of one layer (one elected thread): D = A * W^T over K.
 template <int N, int K>
 __device__ __forceinline__ void issue_layer(uint32_t d, uint32_t a_s, uint32_t w_s) {
@@ -112,21 +137,85 @@ __device__ __forceinline__ void issue_layer(uint32_t d, uint32_t a_s, uint32_t w
     tc::mma_bf16(d, tc::sdesc(a_s + 256 * s, 128, sbo), tc::sdesc(w_s + 256 * s, 128, sbo), id, s > 0 ? 1u : 0u);
 }
 
+// As issue_layer, then one more K = 16 slice that adds the bias: A = the
+// tile of ones (columns 0..2), B = the layer's bias tile (three bf16 pieces
+// per output in columns 0..2).
+template <int N, int K>
+__device__ __forceinline__ void issue_layer_bias(uint32_t d, uint32_t a_s, uint32_t w_s, uint32_t ones_s,
+                                                 uint32_t bias_s) {
+  issue_layer<N, K>(d, a_s, w_s);
+  tc::mma_bf16(d, tc::sdesc(ones_s, 128, 256), tc::sdesc(bias_s, 128, 256), tc::idesc_bf16(128, N, false, false), 1u);
+}
+
+// Per-CTA folds of the inference copy of the parameters (the training
+// kernels keep MlpDev as the host wrote it):
+//  * the biases enter the accumulators through the tensor cores.  Each f32
+//    bias b is split into bf16 pieces hi + mid + lo (24 bits: b itself);
+//    layer 1 reads them from W1 columns 13..15 against feature columns
+//    13..15 set to one in the A tile, layers 2..4 from a bias tile [N][16]
+//    against a shared tile of ones [128][16] (kInferBiasBytes);
+//  * W2, W3, W4 are halved for the doubled GELU of hidden_epilogue_infer.
+// Ends with the proxy fence that makes these shared-memory writes, and the
+// parameter copy before them, visible to the tensor cores.
+constexpr int kInferBiasBytes = 4096 + 2048 + 2048 + 512;  // ones, bias tiles of layers 2, 3, 4
+constexpr uint32_t kBf16One = 0x3F80u;
+
+__device__ __forceinline__ void bias_pieces(float b, __nv_bfloat16 (&pc)[3]) {
+  pc[0] = __float2bfloat16_rn(b);
+  const float r1 = b - __bfloat162float(pc[0]);
+  pc[1] = __float2bfloat16_rn(r1);
+  pc[2] = __float2bfloat16_rn(r1 - __bfloat162float(pc[1]));
+}
+
+__device__ __forceinline__ void infer_prologue(MlpDev* P, unsigned char* tiles) {
+  const __nv_bfloat162 h2 = __floats2bfloat162_rn(0.5f, 0.5f);
+  __nv_bfloat162* w2 = reinterpret_cast<__nv_bfloat162*>(P->w2);
+  __nv_bfloat162* w3 = reinterpret_cast<__nv_bfloat162*>(P->w3);
+  __nv_bfloat162* w4 = reinterpret_cast<__nv_bfloat162*>(P->w4);
+  for (int i = threadIdx.x; i < 64 * 64 / 2; i += blockDim.x) { w2[i] = __hmul2(w2[i], h2); w3[i] = __hmul2(w3[i], h2); }
+  for (int i = threadIdx.x; i < 16 * 64 / 2; i += blockDim.x) w4[i] = __hmul2(w4[i], h2);
+  __nv_bfloat16* ones = reinterpret_cast<__nv_bfloat16*>(tiles);
+  __nv_bfloat16* bt[3] = {ones + 128 * 16, ones + 128 * 16 + 64 * 16, ones + 128 * 16 + 2 * 64 * 16};
+  const float* bsrc[3] = {P->b2, P->b3, P->b4};
+  const int nrow[3] = {64, 64, 16};
+  for (int i = threadIdx.x; i < 128 * 16; i += blockDim.x) {
+    const int row = i >> 4, k = i & 15;
+    ones[tc::tile_elem(row, k, 16)] = __float2bfloat16_rn(k < 3 ? 1.0f : 0.0f);
+  }
+#pragma unroll
+  for (int l = 0; l < 3; l++)
+    for (int i = threadIdx.x; i < nrow[l] * 16; i += blockDim.x) {
+      const int row = i >> 4, k = i & 15;
+      __nv_bfloat16 pc[3];
+      bias_pieces(bsrc[l][row], pc);
+      bt[l][tc::tile_elem(row, k, 16)] = k < 3 ? pc[k] : __float2bfloat16_rn(0.0f);
+    }
+  for (int o = threadIdx.x; o < 64; o += blockDim.x) {
+    __nv_bfloat16 pc[3];
+    bias_pieces(P->b1[o], pc);
+#pragma unroll
+    for (int k = 0; k < 3; k++) P->w1[tc::tile_elem(o, 13 + k, 16)] = pc[k];
+  }
+  tc::fence_async_smem();
+}
+
 // ------------------------------------------------------------------------
 // Inference.  G groups of 4 warps per CTA, each group owns one tile at a
 // time, 64 tensor-memory columns and one 16 KB activation tile; the groups'
 // epilogues overlap each other's MMAs.  Features: bf16 [n][16] (columns
-// 0..10 normalised inputs; 11..15 are multiplied by the zero-padded columns
-// of W1, so they may carry data for the epilogue).  out(p, valid, y, f0, f1,
+// 0..10 normalised inputs; 11 and 12 meet zero columns of W1, so they may
+// carry data for the epilogue; 13..15 are read as ones by the tensor cores,
+// against the bias pieces of infer_prologue).  out(p, valid, y, f0, f1,
 // P) consumes the 16 output columns (y[0..5] normalised outputs + biases)
 // and returns three terms summed per CTA into dissip_part[3 blockIdx.x + j],
 // j = 0, 1, 2 (when non-null).
 // ------------------------------------------------------------------------
 constexpr int kInferGroups = 4;
 constexpr int kInferCtasPerSm = 2;  // 2 x 256 tensor-memory columns, 2 x 87 KB shared memory
-// after the activation tiles: G mbarriers, the tensor-memory slot and three
+// after the activation tiles: the tile of ones and the bias tiles
+// (kInferBiasBytes), then G mbarriers, the tensor-memory slot and three
 // doubles per warp for the per-CTA sums (40 + 384 bytes at 16 warps)
-constexpr size_t kInferSmem = sizeof(MlpDev) + (size_t)kInferGroups * 16384 + 512;
+constexpr size_t kInferSmem = sizeof(MlpDev) + (size_t)kInferGroups * 16384 + kInferBiasBytes + 512;
 
 // One group's view of its tile: shared-memory addresses of its activation
 // tile and of the weight tiles, its 64 tensor-memory columns, its named
@@ -134,13 +223,14 @@ constexpr size_t kInferSmem = sizeof(MlpDev) + (size_t)kInferGroups * 16384 + 51
 struct MlpGroup {
   unsigned char* act;
   uint32_t act_s, w1s, w2s, w3s, w4s, dcol, my_t;
+  uint32_t ones_s, b2s, b3s, b4s;  // inference: tile of ones and bias tiles
   int bar;
   uint64_t* mbar;
   uint32_t parity;
 };
 
-__device__ __forceinline__ MlpGroup mlp_group(MlpDev* P, unsigned char* act, uint32_t tbase, int g, int q,
-                                              uint64_t* mbar) {
+__device__ __forceinline__ MlpGroup mlp_group(MlpDev* P, unsigned char* act, unsigned char* tiles, uint32_t tbase,
+                                              int g, int q, uint64_t* mbar) {
   MlpGroup G;
   G.act = act;
   G.act_s = tc::smem_addr(act);
@@ -148,6 +238,10 @@ __device__ __forceinline__ MlpGroup mlp_group(MlpDev* P, unsigned char* act, uin
   G.w2s = tc::smem_addr(P->w2);
   G.w3s = tc::smem_addr(P->w3);
   G.w4s = tc::smem_addr(P->w4);
+  G.ones_s = tc::smem_addr(tiles);
+  G.b2s = G.ones_s + 4096;
+  G.b3s = G.ones_s + 6144;
+  G.b4s = G.ones_s + 8192;
   G.dcol = tbase + 64 * g;
   G.my_t = G.dcol + ((uint32_t)(q * 32) << 16);
   G.bar = 1 + g;
@@ -158,8 +252,9 @@ __device__ __forceinline__ MlpGroup mlp_group(MlpDev* P, unsigned char* act, uin
 
 // The network on one 128-sample tile by one group of 4 warps (thread r owns
 // sample r): features f0, f1 (bf16 x 16) in, the 16 output columns of this
-// sample's lane (outputs + b4) out.  Returns false in every thread of the
-// group when an MMA did not complete within its wait limit.
+// sample's lane (outputs + b4) out, with the parameters as infer_prologue
+// folded them.  Returns false in every thread of the group when an MMA did
+// not complete within its wait limit.
 __device__ __forceinline__ bool mlp_tile(MlpGroup& G, const MlpDev* P, int r, uint4 f0, uint4 f1,
                                          float (&y)[16]) {
   auto wait_mma = [&]() -> bool {
@@ -168,8 +263,10 @@ __device__ __forceinline__ bool mlp_tile(MlpGroup& G, const MlpDev* P, int r, ui
     tc::fence_after_sync();
     return ok;
   };
+  // feature columns 13..15 read as ones (they meet the bias pieces in W1)
+  const uint4 f1a = make_uint4(f1.x, f1.y, (f1.z & 0xFFFFu) | (kBf16One << 16), kBf16One | (kBf16One << 16));
   *reinterpret_cast<uint4*>(G.act + 2 * tc::tile_elem(r, 0, 16)) = f0;
-  *reinterpret_cast<uint4*>(G.act + 2 * tc::tile_elem(r, 8, 16)) = f1;
+  *reinterpret_cast<uint4*>(G.act + 2 * tc::tile_elem(r, 8, 16)) = f1a;
   tc::fence_async_smem();
   tc::fence_before_sync();
   tc::bar_sync(G.bar, 128);
@@ -179,39 +276,37 @@ __device__ __forceinline__ bool mlp_tile(MlpGroup& G, const MlpDev* P, int r, ui
     tc::mma_commit(G.mbar);
   }
   bool bad = !wait_mma();
-  hidden_epilogue(G.my_t, P->b1, G.act, r);
+  hidden_epilogue_infer(G.my_t, G.act, r);
   tc::fence_async_smem();
   tc::fence_before_sync();
   if (bar_any(G.bar, 128, bad)) return false;
   if (r == 0) {
     tc::fence_after_sync();
-    issue_layer<64, 64>(G.dcol, G.act_s, G.w2s);
+    issue_layer_bias<64, 64>(G.dcol, G.act_s, G.w2s, G.ones_s, G.b2s);
     tc::mma_commit(G.mbar);
   }
   bad = !wait_mma();
-  hidden_epilogue(G.my_t, P->b2, G.act, r);
+  hidden_epilogue_infer(G.my_t, G.act, r);
   tc::fence_async_smem();
   tc::fence_before_sync();
   if (bar_any(G.bar, 128, bad)) return false;
   if (r == 0) {
     tc::fence_after_sync();
-    issue_layer<64, 64>(G.dcol, G.act_s, G.w3s);
+    issue_layer_bias<64, 64>(G.dcol, G.act_s, G.w3s, G.ones_s, G.b3s);
     tc::mma_commit(G.mbar);
   }
   bad = !wait_mma();
-  hidden_epilogue(G.my_t, P->b3, G.act, r);
+  hidden_epilogue_infer(G.my_t, G.act, r);
   tc::fence_async_smem();
   tc::fence_before_sync();
   if (bar_any(G.bar, 128, bad)) return false;
   if (r == 0) {
     tc::fence_after_sync();
-    issue_layer<16, 64>(G.dcol, G.act_s, G.w4s);
+    issue_layer_bias<16, 64>(G.dcol, G.act_s, G.w4s, G.ones_s, G.b4s);
     tc::mma_commit(G.mbar);
   }
   bad = !wait_mma();
   tc::tmem_ld16(G.my_t, y);
-#pragma unroll
-  for (int j = 0; j < 16; j++) y[j] += P->b4[j];
   tc::fence_before_sync();
   return !bar_any(G.bar, 128, bad);
 }
@@ -233,13 +328,16 @@ k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long
   extern __shared__ __align__(1024) unsigned char smraw_tc[];
   MlpDev* P = reinterpret_cast<MlpDev*>(smraw_tc);
   unsigned char* act_all = smraw_tc + sizeof(MlpDev);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(act_all + (size_t)G * 16384);
+  unsigned char* tiles = act_all + (size_t)G * 16384;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + kInferBiasBytes);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + G);
   double* red = reinterpret_cast<double*>(bars + G + 1);
 
   const int tid = threadIdx.x, g = tid >> 7, r = tid & 127, warp = tid >> 5, q = warp & 3;
   for (int i = tid; i < (int)(sizeof(MlpDev) / 16); i += blockDim.x)
     reinterpret_cast<uint4*>(P)[i] = reinterpret_cast<const uint4*>(prm)[i];
+  __syncthreads();
+  infer_prologue(P, tiles);
   if (tid < G) tc::mbar_init(&bars[tid], 1);
   if (warp == 0) {
     tc::tmem_alloc(tslot, 64 * G);
@@ -250,7 +348,7 @@ k_mlp_infer(const MlpDev* __restrict__ prm, const uint4* __restrict__ feat, long
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tbase = *tslot;
-  MlpGroup grp = mlp_group(P, act_all + (size_t)g * 16384, tbase, g, q, &bars[g]);
+  MlpGroup grp = mlp_group(P, act_all + (size_t)g * 16384, tiles, tbase, g, q, &bars[g]);
   double dsum = 0.0, dsum2 = 0.0, dsum3 = 0.0;
   const long long ntiles = (n + 127) / 128;
   for (long long tile = (long long)blockIdx.x * G + g; tile < ntiles; tile += (long long)gridDim.x * G) {
