@@ -559,8 +559,8 @@ struct Engine : EngineBase {
   void learned_features_into(void* feat, bool raw) {
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
-      using C = ColCfg<NN, T>;
-      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::TC / 2), NZ, 3), dim3(C::THREADS), C::buf(), st, (const cx<T>*)uh.p,
+      using C = LgyCfg<NN, T>;
+      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::H), NZ, 3), dim3(C::THREADS), C::smem(), st, (const cx<T>*)uh.p,
              (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)ky0, tw);
     });
     const T inv_h = (T)(2.0 / cfg.zl);

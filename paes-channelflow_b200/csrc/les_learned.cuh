@@ -52,16 +52,23 @@
 
 namespace les {
 
+// Blocks of k_lgrad_y: H = ColCfg's column count (64-byte row segments of
+// the spectra) and 2H transforms, the field and its y derivative.
+template <int N, class T> struct LgyCfg {
+  static constexpr int H = ColCfg<N, T>::TC;
+  static constexpr int THREADS = 2 * H * Split<N>::N2;
+  static constexpr size_t smem() { return (size_t)2 * H * N * sizeof(cx<T>); }
+};
+
 // y-inverse rows gy[f][z][y][kx], f = 0..5: U, UY, V, VY, W, WY.  A block
-// takes H = TC/2 columns of one component (blockIdx.z: u, v, w) at one
-// level and runs 2H transforms: t < H the field, t >= H its y derivative,
-// so each spectral value is read once.
+// takes H columns of one component (blockIdx.z: u, v, w) at one level and
+// runs 2H transforms: t < H the field, t >= H its y derivative, so each
+// spectral value is read from memory once.
 template <class T, int N>
-__global__ void __launch_bounds__(ColCfg<N, T>::THREADS)
+__global__ void __launch_bounds__(LgyCfg<N, T>::THREADS)
 k_lgrad_y(const cx<T>* __restrict__ uh, const cx<T>* __restrict__ vh, const cx<T>* __restrict__ wh,
           cx<T>* __restrict__ gy, int KX, int NZ, T ky0, const cx<T>* __restrict__ tw) {
-  using C = ColCfg<N, T>;
-  constexpr int H = C::TC / 2;
+  constexpr int H = LgyCfg<N, T>::H;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
   const int z = blockIdx.y + 1;
@@ -112,9 +119,17 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
   constexpr int KX = NX / 2, RB = L::RB;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-  const size_t R = (size_t)NZ * NY;
-  const size_t plane = R * KX;
-  const size_t r0 = (size_t)blockIdx.x * RB;
+  const int R = NZ * NY;
+  const size_t plane = (size_t)R * KX;
+  const int r0 = blockIdx.x * RB;
+  // level (0-based) and y of the block's first row; row r0 + rr is at
+  // y0 + rr, carried into the next level past NY - 1 (RB <= NY)
+  const int zb = r0 / NY, y0 = r0 - zb * NY;
+  auto row_zy = [&](int rr, int& z, int& y) {
+    y = y0 + rr;
+    z = zb;
+    if (y >= NY) { y -= NY; z++; }
+  };
   // row of field f at level k (1..NZ) and y
   auto rowp = [&](int f, int k, int y) -> const cx<T>* { return gy + (size_t)f * plane + ((size_t)(k - 1) * NY + y) * KX; };
   // Stage 1: the spectral combinations a + i b of the five transforms of
@@ -125,10 +140,11 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
   for (int i = threadIdx.x; i < 5 * RB * KX; i += blockDim.x) {
     const int t = i / KX, k = i - t * KX;
     const int rr = t / 5, j = t - 5 * rr;
-    const size_t row = r0 + rr;
     cx<T> d = zero_cx<T>(), m = zero_cx<T>();
-    if (row < R) {
-      const int z = (int)(row / NY) + 1, y = (int)(row - (size_t)(z - 1) * NY);
+    if (r0 + rr < R) {
+      int z, y;
+      row_zy(rr, z, y);
+      z += 1;
       const T xk = kx0 * (T)k;
       auto wl = [&](int f, int kk) -> cx<T> { return (kk >= 1 && kk <= NZ - 1) ? rowp(f, kk, y)[k] : zero_cx<T>(); };
       auto vz = [&](int f) -> cx<T> {
@@ -158,10 +174,16 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
     if (NX - n < KX) return zm[(size_t)t * KX + (NX - n)];
     return zero_cx<T>();
   }, NoStore{});
+  // the feature normalisation, read once per thread
+  float nsh[11], nsc[11];
+#pragma unroll
+  for (int jj = 0; jj < 11; jj++) {
+    nsh[jj] = RAW ? 0.f : P->in_shift[jj];
+    nsc[jj] = RAW ? 1.f : P->in_scale[jj];
+  }
   for (int i = threadIdx.x; i < RB * NX; i += blockDim.x) {
     const int rr = i / NX, x = i - rr * NX;
-    const size_t row = r0 + rr;
-    if (row >= R) continue;
+    if (r0 + rr >= R) continue;
     T g[9];
 #pragma unroll
     for (int j = 0; j < 5; j++) {
@@ -169,10 +191,11 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
       g[2 * j] = v.x;
       if (j < 4) g[2 * j + 1] = v.y;
     }
-    const int z = (int)(row / NY);
+    int z, y;
+    row_zy(rr, z, y);
     const T zc = ((T)z + (T)0.5) * dz;
     const T zw = zc < zl - zc ? zc : zl - zc;
-    const size_t p = row * NX + x;
+    const size_t p = (size_t)(r0 + rr) * NX + x;
     T g2 = (T)0;
 #pragma unroll
     for (int j = 0; j < 9; j++) g2 += g[j] * g[j];
@@ -194,7 +217,7 @@ k_lgrad_x(const cx<T>* __restrict__ gy, void* __restrict__ feat, const MlpDev* _
     } else {
       float f[11];
 #pragma unroll
-      for (int jj = 0; jj < 11; jj++) f[jj] = (float)((xin[jj] - (T)P->in_shift[jj]) * (T)P->in_scale[jj]);
+      for (int jj = 0; jj < 11; jj++) f[jj] = (float)((xin[jj] - (T)nsh[jj]) * (T)nsc[jj]);
       const __nv_bfloat16 shi = __float2bfloat16_rn(sc);
       const float slo = sc - __bfloat162float(shi);
       uint4* o = reinterpret_cast<uint4*>(feat) + 2 * p;
