@@ -52,10 +52,11 @@
 
 namespace les {
 
-// Blocks of k_lgrad_y: H = ColCfg's column count (64-byte row segments of
-// the spectra) and 2H transforms, the field and its y derivative.
+// Blocks of k_lgrad_y: H = half of ColCfg's column count and 2H
+// transforms, the field and its y derivative (measured faster on B200 than
+// full-width 64-byte column segments at twice the block size).
 template <int N, class T> struct LgyCfg {
-  static constexpr int H = ColCfg<N, T>::TC;
+  static constexpr int H = ColCfg<N, T>::TC / 2;
   static constexpr int THREADS = 2 * H * Split<N>::N2;
   static constexpr size_t smem() { return (size_t)2 * H * N * sizeof(cx<T>); }
 };

@@ -107,24 +107,13 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* __r
 // a K = 64 activation tile.  The factor 2 is taken back by the halved
 // weights of the next layer (infer_prologue); both scalings are exact in
 // bf16, so the next layer's products equal those of GELU(z) and W.
-template <bool ALU_CVT>
 __device__ __forceinline__ uint32_t gelu2_pack(float a, float b) {
-  __nv_bfloat162 x;
-  if constexpr (ALU_CVT) {
-    // f32 -> bf16 pair on the integer pipe: round half away from zero, then
-    // the high halves (differs from round-to-nearest-even only on exact ties)
-    x = tc::bf2_from(__byte_perm(__float_as_uint(a) + 0x8000u, __float_as_uint(b) + 0x8000u, 0x7632));
-  } else {
-    x = __floats2bfloat162_rn(a, b);
-  }
+  const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
   const __nv_bfloat162 c = __floats2bfloat162_rn(kGeluC, kGeluC);
   const __nv_bfloat162 ca = __floats2bfloat162_rn(kGeluC * kGeluA, kGeluC * kGeluA);
   const __nv_bfloat162 u = __hmul2(x, __hfma2(__hmul2(x, x), ca, c));
   return tc::bf2_bits(__hfma2(x, tc::tanh_bf2(u), x));
 }
-// The conversions of half the columns run on the integer pipe, so that the
-// special-function pipe (tanh and the other half of the conversions) is not
-// the only one that saturates.
 __device__ __forceinline__ void hidden_epilogue_infer(uint32_t taddr, unsigned char* act, int r) {
 #pragma unroll
   for (int c = 0; c < 4; c++) {
@@ -132,8 +121,7 @@ __device__ __forceinline__ void hidden_epilogue_infer(uint32_t taddr, unsigned c
     tc::tmem_ld16(taddr + 16 * c, v);
     uint32_t pk[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++)
-      pk[j] = (c & 1) ? gelu2_pack<true>(v[2 * j], v[2 * j + 1]) : gelu2_pack<false>(v[2 * j], v[2 * j + 1]);
+    for (int j = 0; j < 8; j++) pk[j] = gelu2_pack(v[2 * j], v[2 * j + 1]);
     *reinterpret_cast<uint4*>(act + 2 * tc::tile_elem(r, 16 * c, 64)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     *reinterpret_cast<uint4*>(act + 2 * tc::tile_elem(r, 16 * c + 8, 64)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
   }
