@@ -353,11 +353,11 @@ __device__ __forceinline__ void smem_fft(int ntrans, cx<T>* sm, const cx<T>* __r
 // table itself (e.g. staged in shared memory by stage_twiddles); fft_core
 // reads it from the global table.
 template <int N, int S, bool COLS, bool IN_SMEM, bool OUT_SMEM, class T, class LoadF, class StoreF>
-__device__ __forceinline__ void fft_core_tab(int ntrans, cx<T>* sm, const cx<T>* twn, LoadF load, StoreF store,
-                                             int it = threadIdx.x) {
+__device__ __forceinline__ void fft_core_tab(int ntrans, cx<T>* sm, const cx<T>* twn, LoadF load, StoreF store) {
   constexpr int N1 = Split<N>::N1;
   constexpr int N2 = Split<N>::N2;
   constexpr int LD = N2 + 1;
+  const int it = threadIdx.x;
   {
     const bool active = it < ntrans * N2;
     int t = 0, n2 = 0;
@@ -416,8 +416,8 @@ __device__ __forceinline__ void fft_core_tab(int ntrans, cx<T>* sm, const cx<T>*
 }
 template <int N, int S, bool COLS, bool IN_SMEM, bool OUT_SMEM, class T, class LoadF, class StoreF>
 __device__ __forceinline__ void fft_core(int ntrans, cx<T>* sm, const cx<T>* __restrict__ tw, LoadF load,
-                                         StoreF store, int it = threadIdx.x) {
-  fft_core_tab<N, S, COLS, IN_SMEM, OUT_SMEM, T>(ntrans, sm, tw + tw_off(N), load, store, it);
+                                         StoreF store) {
+  fft_core_tab<N, S, COLS, IN_SMEM, OUT_SMEM, T>(ntrans, sm, tw + tw_off(N), load, store);
 }
 // Copy of the length-N twiddle table into shared memory `dst` (N entries),
 // by the whole block; ends with a barrier.
@@ -434,35 +434,6 @@ struct NoLoad {
 struct NoStore {
   template <class V> __device__ void operator()(int, int, V) const {}
 };
-
-// Asynchronous 16-byte global -> shared copies (cp.async, bypassing L1):
-// the staging of the next tile while the current one is transformed.  The
-// waits are the hardware's group waits: no spinning.
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
-               "l"((unsigned long long)__cvta_generic_to_global(gsrc))
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// wait until at most N of this thread's most recent copy groups are pending
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// The same pointer, opaque to the compiler: loads through it inside a
-// persistent loop are not hoisted out of the loop (which would keep a whole
-// twiddle table in registers across iterations).
-template <class P> __device__ __forceinline__ P* opaque_ptr(P* p) {
-  unsigned long long r;
-  asm volatile("mov.b64 %0, %1;" : "=l"(r) : "l"((unsigned long long)p));
-  return reinterpret_cast<P*>(r);
-}
-// likewise for an index (the thread index inside a persistent loop)
-__device__ __forceinline__ int opaque_int(int v) {
-  int r;
-  asm volatile("mov.b32 %0, %1;" : "=r"(r) : "r"(v));
-  return r;
-}
 
 // Signed wavenumber index of FFT bin k for length n (k > n/2 -> k - n).
 __host__ __device__ __forceinline__ int signed_k(int k, int n) { return (k > n / 2) ? k - n : k; }

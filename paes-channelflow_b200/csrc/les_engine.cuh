@@ -455,9 +455,6 @@ struct Engine : EngineBase {
     if (ree) d2h(re.p, ree, ps * NZ, rb);
   }
 
-  // persistent y-transform kernels: one CTA per SM, at most one per tile
-  unsigned ytile_grid(int TC) const { return (unsigned)std::min(YTiles(KX, TC, NZ).n, nsm); }
-
   // ---- the stage ----
   void comp1_kernels(const StageArgs& a) {
     const T dtab2 = (T)a.dtab2;
@@ -475,12 +472,12 @@ struct Engine : EngineBase {
       using C = ColCfg<N, T>;
       launch(k_col_small<T, N, false>, dim3(cdiv(KX, C::TC), NZ - 1), dim3(C::THREADS), C::buf(), st,
              (const cx<T>*)Xe.p, Xe.p, KX, (T)(1.0 / ((double)NX * NY)), tw);
-      using CI = YInvCfg<T, N>;
+      using CM = ColCfg<3 * N / 2, T>;
       Ptr8 src{}, dst{};
       src.p[0] = uh.p; src.p[1] = vh.p; src.p[2] = wh.p; src.p[3] = Xe.p;
       for (int i = 0; i < 8; i++) dst.p[i] = mixed[i].p;
-      launch(k_y_inverse<T, N>, dim3(ytile_grid(ColCfg<3 * N / 2, T>::TC)), dim3(CI::THREADS), CI::smem(), st, src,
-             dst, KX, NZ, (T)ky0, tw);
+      launch(k_y_inverse<T, N>, dim3(cdiv(KX, CM::TC), NZ, 4), dim3(2 * CM::THREADS), 2 * CM::buf(), st, src, dst,
+             KX, NZ, (T)ky0, tw);
     });
     if (fused) {
       fused_middle(a);

@@ -273,89 +273,35 @@ k_e_prep(T* __restrict__ e, const T* __restrict__ re, cx<T>* __restrict__ Xe, in
 struct Ptr8 { void* p[8]; };
 struct Ptr12 { void* p[12]; };
 
-// Tiles of the persistent y-transform kernels: (TC-column group, level,
-// field) with the column group fastest; u, v have NZ levels, w, e NZ - 1.
-struct YTiles {
-  int KXT, NZ, per_uv, per_we, n;
-  __host__ __device__ YTiles(int KX, int TC, int NZ_) : KXT((KX + TC - 1) / TC), NZ(NZ_) {
-    per_uv = NZ * KXT;
-    per_we = (NZ - 1) * KXT;
-    n = 2 * per_uv + 2 * per_we;
-  }
-  __device__ void decode(int idx, int TC, int& f, int& z, int& kx0) const {
-    int r;
-    if (idx < 2 * per_uv) { f = idx / per_uv; r = idx - f * per_uv; }
-    else { idx -= 2 * per_uv; f = 2 + idx / per_we; r = idx - (f - 2) * per_we; }
-    z = r / KXT + 1;
-    kx0 = (r - (z - 1) * KXT) * TC;
-  }
-};
-
 // expand() of u, v, w, e in y fused with d/dy: for field f (u, v, w, e),
 // out[2f] = IFFT_M(pad(s)), out[2f+1] = IFFT_M(i*ky*pad(s)), computed as one
-// batch of 2*TC transforms per tile from the tile's NS x TC spectral
-// columns.  Persistent: each CTA walks the tiles with a stride of gridDim.x,
-// and the columns of its next tile are copied into shared memory
-// (cp.async, two staging buffers) while the current tile is transformed.
-// Shared memory: the transform buffer (2 TC M) and two staging buffers
-// (NS TC each).
+// batch of 2*TC transforms (the second half re-reads the same columns from
+// L1).  blockIdx.z = f.
 template <class T, int NS>
 __global__ void __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS * 2)
 k_y_inverse(Ptr8 src, Ptr8 dst, int KX, int NZ, T ky0, const cx<T>* __restrict__ tw) {
   constexpr int M = 3 * NS / 2;
   using C = ColCfg<M, T>;
-  constexpr int TC = C::TC, TC2 = 2 * TC;
-  constexpr int EPC = 16 / (int)sizeof(cx<T>);  // complex values per 16-byte chunk
-  constexpr int CPR = TC / EPC;                  // chunks per row segment
-  static_assert(TC % EPC == 0, "row segments of whole 16-byte chunks");
+  constexpr int TC2 = 2 * C::TC;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-  cx<T>* stg0 = sm + (size_t)TC2 * M;
-  const YTiles tiles(KX, TC, NZ);
-  auto issue = [&](int idx, cx<T>* stg) {
-    int f, z, kx0;
-    tiles.decode(idx, TC, f, z, kx0);
-    const cx<T>* in = reinterpret_cast<const cx<T>*>(src.p[f]) + (size_t)(z - 1) * NS * KX + kx0;
-    for (int i = threadIdx.x; i < NS * CPR; i += blockDim.x) {
-      const int ky = i / CPR, c = i - ky * CPR;
-      if (kx0 + c * EPC < KX) cp_async16(stg + (size_t)ky * TC + c * EPC, in + (size_t)ky * KX + c * EPC);
-    }
-  };
-  int tile = blockIdx.x;
-  if (tile < tiles.n) issue(tile, stg0);
-  cp_async_commit();
-#pragma unroll 1
-  for (int it = 0; tile < tiles.n; tile += gridDim.x, it++) {
-    const cx<T>* stg = stg0 + (size_t)(it & 1) * NS * TC;
-    if (tile + (int)gridDim.x < tiles.n) issue(tile + gridDim.x, stg0 + (size_t)((it + 1) & 1) * NS * TC);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
-    int f, z, kx0;
-    tiles.decode(tile, TC, f, z, kx0);
-    cx<T>* out0 = reinterpret_cast<cx<T>*>(dst.p[2 * f]) + (size_t)(z - 1) * M * KX;
-    cx<T>* out1 = reinterpret_cast<cx<T>*>(dst.p[2 * f + 1]) + (size_t)(z - 1) * M * KX;
-    // the twiddle table and the thread index made opaque, so that the
-    // compiler keeps none of the transform's loop-invariant loads and
-    // indexes in registers across tiles
-    fft_core<M, +1, true, false, false>(TC2, sm, opaque_ptr(tw), [&](int t, int n) {
-      const int tt = t % TC, kx = kx0 + tt;
-      const int ky = (n < NS / 2) ? n : ((n > NS) ? n - NS / 2 : -1);
-      cx<T> v = (kx < KX && ky >= 0) ? stg[(size_t)ky * TC + tt] : zero_cx<T>();
-      if (t >= TC) v = mul_i(v) * (ky0 * (T)signed_k(n, M));
-      return v;
-    }, [&](int t, int n, cx<T> v) {
-      const int tt = t % TC, kx = kx0 + tt;
-      if (kx < KX) (t < TC ? out0 : out1)[(size_t)n * KX + kx] = v;
-    }, opaque_int(threadIdx.x));
-    __syncthreads();
-  }
+  const int f = blockIdx.z, z = blockIdx.y + 1;
+  if (f >= 2 && z == NZ) return;
+  const int kx0 = blockIdx.x * C::TC;
+  const cx<T>* in = reinterpret_cast<const cx<T>*>(src.p[f]) + (size_t)(z - 1) * NS * KX;
+  cx<T>* out0 = reinterpret_cast<cx<T>*>(dst.p[2 * f]) + (size_t)(z - 1) * M * KX;
+  cx<T>* out1 = reinterpret_cast<cx<T>*>(dst.p[2 * f + 1]) + (size_t)(z - 1) * M * KX;
+  fft_core<M, +1, true, false, false>(TC2, sm, tw, [&](int t, int n) {
+    const int tt = t % C::TC, kx = kx0 + tt;
+    const int ky = (n < NS / 2) ? n : ((n > NS) ? n - NS / 2 : -1);
+    cx<T> v = (kx < KX && ky >= 0) ? in[(size_t)ky * KX + kx] : zero_cx<T>();
+    if (t >= C::TC) v = mul_i(v) * (ky0 * (T)signed_k(n, M));
+    return v;
+  }, [&](int t, int n, cx<T> v) {
+    const int tt = t % C::TC, kx = kx0 + tt;
+    if (kx < KX) (t < C::TC ? out0 : out1)[(size_t)n * KX + kx] = v;
+  });
 }
-template <class T, int NS> struct YInvCfg {
-  using C = ColCfg<3 * NS / 2, T>;
-  static constexpr int THREADS = 2 * C::THREADS;
-  static constexpr size_t smem() { return (2 * (size_t)C::TC * (3 * NS / 2) + 2 * (size_t)NS * C::TC) * sizeof(cx<T>); }
-};
 
 // expand() in x fused with d/dx: six paired inverse row transforms give
 // U,UX | V,VX | W,WX | UY,VY | WY,E | EX,EY on the padded grid.
