@@ -249,7 +249,10 @@ def run_form(P, precision, steps, warmup, dev, want_profile, imodel=3, mlp=None,
 
 def run_e2e(P, steps, dev, precision, imodel=3, mlp=None):
     """Through the C ABI with host buffers: upload the state from pinned host
-    memory, then steps x (les_gpu_step + les_gpu_stats read-back)."""
+    memory, then steps x (les_gpu_step + les_gpu_stats read-back).  The host
+    arrays hold the form's own reals: 8 bytes for the FP64 form, 4 for the
+    mixed forms (the reference as shipped keeps u, v, w, e, p in 4-byte
+    reals; FP64 is its -fdefault-real-8 build)."""
     import torch
     cfg = P.channel_config(NX, NY, NZ, dt=1e-3, re_tau=RE_TAU, precision=precision, device=dev, imodel=imodel)
     g = P.LesGpu(cfg)
@@ -258,7 +261,8 @@ def run_e2e(P, steps, dev, precision, imodel=3, mlp=None):
     g.make_ic(seed=12345, amp=0.1, re_tau=RE_TAU)
     dt = g.cfl_dt(0.5)
     shape = (NZ, NY, NX)
-    host = {k: torch.empty(shape, dtype=torch.float64, pin_memory=True) for k in "uvwep"}
+    hdt = torch.float64 if precision == 8 else torch.float32
+    host = {k: torch.empty(shape, dtype=hdt, pin_memory=True) for k in "uvwep"}
     g.download_into(*[host[k] for k in "uvwep"])
     g.step(it=1, mnout=False, dt=dt)  # build the step graph outside the timed region
     g.stats()
@@ -498,8 +502,8 @@ def main():
                   "learned_mixed_sign_test_only_used_fraction": rs["stages_used"] / max(rs["stages_timed"], 1)},
         "errors": {"learned_mixed_vs_fp64": errors(rl), "mixed_vs_fp64": errors(r32)},
         "e2e": {"value": e2e, "unit": "Mpoint-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "mode": "device-resident drop-in: state uploaded once inside the timed region, statistics read "
-                        "back every step"},
+                "mode": "device-resident drop-in: state (4-byte host reals, as the shipped reference keeps them) "
+                        "uploaded once inside the timed region, statistics read back every step"},
         "gpu_launches": rl["launches"],
         "clocks": rl["clocks"],
         "roofline": {"bound": "hbm", "kernel": kfull, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -24,15 +24,24 @@ template <class T> __host__ __device__ __forceinline__ cx<T> mk(T a, T b) { cx<T
 template <class T> __device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) { return mk(a.x + b.x, a.y + b.y); }
 template <class T> __device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) { return mk(a.x - b.x, a.y - b.y); }
 template <class T> __device__ __forceinline__ cx<T> operator*(cx<T> a, T s) { return mk(a.x * s, a.y * s); }
-// FP32 complex sums and differences as one packed f32x2 instruction each
-// (sm_100a; each component rounded to nearest as the scalar form): the
-// butterflies of every FP32 transform issue half the additions.
+// FP32 complex sums, differences and real scalings as one packed f32x2
+// instruction each (sm_100a; each component rounded to nearest as the
+// scalar form): the butterflies of every FP32 transform issue half the
+// additions.
 template <> __device__ __forceinline__ cx<float> operator+<float>(cx<float> a, cx<float> b) {
   cx<float> r;
   asm("{\n\t.reg .b64 a, b, r;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
       "add.rn.f32x2 r, a, b;\n\tmov.b64 {%0, %1}, r;\n\t}"
       : "=f"(r.x), "=f"(r.y)
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+template <> __device__ __forceinline__ cx<float> operator*<float>(cx<float> a, float sc) {
+  cx<float> r;
+  asm("{\n\t.reg .b64 a, b, r;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %4};\n\t"
+      "mul.rn.f32x2 r, a, b;\n\tmov.b64 {%0, %1}, r;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(sc));
   return r;
 }
 template <> __device__ __forceinline__ cx<float> operator-<float>(cx<float> a, cx<float> b) {
