@@ -219,6 +219,17 @@ template <int NSX> struct FusedCfg {
   }
 };
 
+// Square root of the TKE in the FP32 form: the hardware approximation
+// (sqrt.approx.f32) instead of the correctly rounded sequence, 3% of the
+// fused kernel (the mixed-form tolerances against the oracle bound its
+// effect); FP64 keeps sqrt().
+template <class T> __device__ __forceinline__ T tke_sqrt(T e) { return sqrt(e); }
+template <> __device__ __forceinline__ float tke_sqrt<float>(float e) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(e));
+  return r;
+}
+
 template <class T, int NSX>
 __global__ void __launch_bounds__(FusedCfg<NSX>::template threads<T>(), (sizeof(T) == 4) ? 2 : 1)
 k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
@@ -295,7 +306,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
     for (int x = lane; x < MX; x += TEAM) we[S(x)].y = tmax(we[S(x)].y, emin);
     team_sync<TEAM>(bar);
   };
-  auto xkk = [&](T e) { return tmin(c01 * sqrt(e), xkmax) + nu; };
+  auto xkk = [&](T e) { return tmin(c01 * tke_sqrt(e), xkmax) + nu; };
 
   // ---- prologue: slots for levels z0-1 and z0, carried tuw/tvw of z0-1 ----
   int sm1 = 0, s0 = 1, sp1 = 2;  // slots of z-1, z, z+1
@@ -439,7 +450,7 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
         const T F = (T)0.5 * E0 * (U0 + U1) - (T)2 * xk0 * exy.x;
         const T H = (T)0.5 * E0 * (V0 + V1) - (T)2 * xk0 * exy.y;
         const T Pe = -(W1 * E1 - Wm * Em) * todzm +
-                     ((xkp + xk0) * (E1 - E0) - (xk0 + xkm) * (E0 - Em)) * (T)a.dzm2 - (T)a.ceps * E0 * sqrt(E0);
+                     ((xkp + xk0) * (E1 - E0) - (xk0 + xkm) * (E0 - Em)) * (T)a.dzm2 - (T)a.ceps * E0 * tke_sqrt(E0);
         work[2][S(x)] = mk(C, G);
         work[3][S(x)] = mk(D, Pw);
         work[4][S(x)] = mk(F, Pe);
