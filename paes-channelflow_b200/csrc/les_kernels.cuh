@@ -274,32 +274,33 @@ struct Ptr8 { void* p[8]; };
 struct Ptr12 { void* p[12]; };
 
 // expand() of u, v, w, e in y fused with d/dy: for field f (u, v, w, e),
-// out[2f] = IFFT_M(pad(s)), out[2f+1] = IFFT_M(i*ky*pad(s)), computed as one
-// batch of 2*TC transforms (the second half re-reads the same columns from
-// L1).  blockIdx.z = f.
+// out[2f] = IFFT_M(pad(s)) (blockIdx.z = 2f) and out[2f+1] =
+// IFFT_M(i*ky*pad(s)) (blockIdx.z = 2f+1), TC columns per block.  The field
+// and its derivative go to separate blocks (the second reads the same
+// columns, mostly from L2): half the block of a paired form, so that two
+// blocks share an SM and one's loads overlap the other's transform and
+// stores (measured 22% faster in FP32 than TC paired transforms per block).
 template <class T, int NS>
-__global__ void __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS * 2)
+__global__ void __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS)
 k_y_inverse(Ptr8 src, Ptr8 dst, int KX, int NZ, T ky0, const cx<T>* __restrict__ tw) {
   constexpr int M = 3 * NS / 2;
   using C = ColCfg<M, T>;
-  constexpr int TC2 = 2 * C::TC;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-  const int f = blockIdx.z, z = blockIdx.y + 1;
+  const int f = blockIdx.z >> 1, h = blockIdx.z & 1, z = blockIdx.y + 1;
   if (f >= 2 && z == NZ) return;
   const int kx0 = blockIdx.x * C::TC;
   const cx<T>* in = reinterpret_cast<const cx<T>*>(src.p[f]) + (size_t)(z - 1) * NS * KX;
-  cx<T>* out0 = reinterpret_cast<cx<T>*>(dst.p[2 * f]) + (size_t)(z - 1) * M * KX;
-  cx<T>* out1 = reinterpret_cast<cx<T>*>(dst.p[2 * f + 1]) + (size_t)(z - 1) * M * KX;
-  fft_core<M, +1, true, false, false>(TC2, sm, tw, [&](int t, int n) {
-    const int tt = t % C::TC, kx = kx0 + tt;
+  cx<T>* out = reinterpret_cast<cx<T>*>(dst.p[2 * f + h]) + (size_t)(z - 1) * M * KX;
+  fft_core<M, +1, true, false, false>(C::TC, sm, tw, [&](int t, int n) {
+    const int kx = kx0 + t;
     const int ky = (n < NS / 2) ? n : ((n > NS) ? n - NS / 2 : -1);
     cx<T> v = (kx < KX && ky >= 0) ? in[(size_t)ky * KX + kx] : zero_cx<T>();
-    if (t >= C::TC) v = mul_i(v) * (ky0 * (T)signed_k(n, M));
+    if (h) v = mul_i(v) * (ky0 * (T)signed_k(n, M));
     return v;
   }, [&](int t, int n, cx<T> v) {
-    const int tt = t % C::TC, kx = kx0 + tt;
-    if (kx < KX) (t < C::TC ? out0 : out1)[(size_t)n * KX + kx] = v;
+    const int kx = kx0 + t;
+    if (kx < KX) out[(size_t)n * KX + kx] = v;
   });
 }
 
