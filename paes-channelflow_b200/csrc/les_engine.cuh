@@ -476,7 +476,7 @@ struct Engine : EngineBase {
       Ptr8 src{}, dst{};
       src.p[0] = uh.p; src.p[1] = vh.p; src.p[2] = wh.p; src.p[3] = Xe.p;
       for (int i = 0; i < 8; i++) dst.p[i] = mixed[i].p;
-      launch(k_y_inverse<T, N>, dim3(cdiv(KX, CM::TC), NZ, 8), dim3(CM::THREADS), CM::buf(), st, src, dst,
+      launch(k_y_inverse<T, N>, dim3(2 * cdiv(KX, CM::TC), NZ, 4), dim3(CM::THREADS), CM::buf(), st, src, dst,
              KX, NZ, (T)ky0, tw);
     });
     if (fused) {

@@ -273,13 +273,13 @@ k_e_prep(T* __restrict__ e, const T* __restrict__ re, cx<T>* __restrict__ Xe, in
 struct Ptr8 { void* p[8]; };
 struct Ptr12 { void* p[12]; };
 
-// expand() of u, v, w, e in y fused with d/dy: for field f (u, v, w, e),
-// out[2f] = IFFT_M(pad(s)) (blockIdx.z = 2f) and out[2f+1] =
-// IFFT_M(i*ky*pad(s)) (blockIdx.z = 2f+1), TC columns per block.  The field
-// and its derivative go to separate blocks (the second reads the same
-// columns, mostly from L2): half the block of a paired form, so that two
-// blocks share an SM and one's loads overlap the other's transform and
-// stores (measured 22% faster in FP32 than TC paired transforms per block).
+// expand() of u, v, w, e in y fused with d/dy: for field f = blockIdx.z
+// (u, v, w, e), out[2f] = IFFT_M(pad(s)) and out[2f+1] = IFFT_M(i*ky*pad(s)),
+// TC columns per block.  The field and its derivative go to separate blocks
+// (h = blockIdx.x & 1), adjacent in launch order so that the second reads
+// the columns from L2: half the block of a paired form, so that two blocks
+// share an SM and one's loads overlap the other's transform and stores
+// (measured 22% faster in FP32 than TC paired transforms per block).
 template <class T, int NS>
 __global__ void __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS)
 k_y_inverse(Ptr8 src, Ptr8 dst, int KX, int NZ, T ky0, const cx<T>* __restrict__ tw) {
@@ -287,9 +287,9 @@ k_y_inverse(Ptr8 src, Ptr8 dst, int KX, int NZ, T ky0, const cx<T>* __restrict__
   using C = ColCfg<M, T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-  const int f = blockIdx.z >> 1, h = blockIdx.z & 1, z = blockIdx.y + 1;
+  const int f = blockIdx.z, h = blockIdx.x & 1, z = blockIdx.y + 1;
   if (f >= 2 && z == NZ) return;
-  const int kx0 = blockIdx.x * C::TC;
+  const int kx0 = (blockIdx.x >> 1) * C::TC;
   const cx<T>* in = reinterpret_cast<const cx<T>*>(src.p[f]) + (size_t)(z - 1) * NS * KX;
   cx<T>* out = reinterpret_cast<cx<T>*>(dst.p[2 * f + h]) + (size_t)(z - 1) * M * KX;
   fft_core<M, +1, true, false, false>(C::TC, sm, tw, [&](int t, int n) {
