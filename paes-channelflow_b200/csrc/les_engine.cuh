@@ -560,7 +560,7 @@ struct Engine : EngineBase {
     with_small(NY, [&](auto cn) {
       constexpr int NN = decltype(cn)::value;
       using C = LgyCfg<NN, T>;
-      launch(k_lgrad_y<T, NN>, dim3(cdiv(KX, C::H), NZ, 3), dim3(C::THREADS), C::smem(), st, (const cx<T>*)uh.p,
+      launch(k_lgrad_y<T, NN>, dim3(2 * cdiv(KX, C::H), NZ, 3), dim3(C::THREADS), C::smem(), st, (const cx<T>*)uh.p,
              (const cx<T>*)vh.p, (const cx<T>*)wh.p, lgy.p, KX, NZ, (T)ky0, tw);
     });
     const T inv_h = (T)(2.0 / cfg.zl);

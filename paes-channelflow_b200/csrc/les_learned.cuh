@@ -52,19 +52,19 @@
 
 namespace les {
 
-// Blocks of k_lgrad_y: H = half of ColCfg's column count and 2H
-// transforms, the field and its y derivative (measured faster on B200 than
-// full-width 64-byte column segments at twice the block size).
+// Blocks of k_lgrad_y: H = ColCfg's column count (64-byte row segments of
+// the spectra), H transforms: the field or its y derivative.
 template <int N, class T> struct LgyCfg {
-  static constexpr int H = ColCfg<N, T>::TC / 2;
-  static constexpr int THREADS = 2 * H * Split<N>::N2;
-  static constexpr size_t smem() { return (size_t)2 * H * N * sizeof(cx<T>); }
+  static constexpr int H = ColCfg<N, T>::TC;
+  static constexpr int THREADS = H * Split<N>::N2;
+  static constexpr size_t smem() { return (size_t)H * N * sizeof(cx<T>); }
 };
 
 // y-inverse rows gy[f][z][y][kx], f = 0..5: U, UY, V, VY, W, WY.  A block
 // takes H columns of one component (blockIdx.z: u, v, w) at one level and
-// runs 2H transforms: t < H the field, t >= H its y derivative, so each
-// spectral value is read from memory once.
+// transforms the field (d = blockIdx.x & 1 = 0) or its y derivative (d = 1);
+// the two blocks of a column group are adjacent in launch order, so the
+// second reads the spectral values from L2.
 template <class T, int N>
 __global__ void __launch_bounds__(LgyCfg<N, T>::THREADS)
 k_lgrad_y(const cx<T>* __restrict__ uh, const cx<T>* __restrict__ vh, const cx<T>* __restrict__ wh,
@@ -73,20 +73,20 @@ k_lgrad_y(const cx<T>* __restrict__ uh, const cx<T>* __restrict__ vh, const cx<T
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
   const int z = blockIdx.y + 1;
-  const int c = blockIdx.z;
-  const int c0 = blockIdx.x * H;
+  const int c = blockIdx.z, d = blockIdx.x & 1;
+  const int c0 = (blockIdx.x >> 1) * H;
   const size_t nm = (size_t)N * KX;
   const cx<T>* src = (c == 0 ? uh : (c == 1 ? vh : wh)) + (size_t)(z - 1) * nm;
   const bool zero = (c == 2 && z == NZ);  // w(nnz) = 0
-  fft_core<N, +1, true, false, false>(2 * H, sm, tw, [&](int t, int n) -> cx<T> {
-    const int kx = c0 + (t < H ? t : t - H);
+  cx<T>* out = gy + ((size_t)(2 * c + d) * NZ + (z - 1)) * nm;
+  fft_core<N, +1, true, false, false>(H, sm, tw, [&](int t, int n) -> cx<T> {
+    const int kx = c0 + t;
     if (kx >= KX || n == N / 2 || zero) return zero_cx<T>();
     const cx<T> v = src[(size_t)n * KX + kx];
-    return t >= H ? mul_i(v) * (ky0 * (T)signed_k(n, N)) : v;
+    return d ? mul_i(v) * (ky0 * (T)signed_k(n, N)) : v;
   }, [&](int t, int k, cx<T> v) {
-    const int kx = c0 + (t < H ? t : t - H);
-    const int f = 2 * c + (t < H ? 0 : 1);
-    if (kx < KX) gy[((size_t)f * NZ + (z - 1)) * nm + (size_t)k * KX + kx] = v;
+    const int kx = c0 + t;
+    if (kx < KX) out[(size_t)k * KX + kx] = v;
   });
 }
 
