@@ -771,15 +771,34 @@ struct Engine : EngineBase {
     fa.dEX = dEX.p; fa.dEY = dEY.p; fa.clipflag = clipflag.p; fa.wp = wp.p;
     fa.divpart = divpart.p; fa.sgspart = sgspart.p;
     fa.lflag = learned_on() ? lflag.p : nullptr;
-    int nch = (int)cdiv(8 * 148, MY);
-    nch = std::max(1, std::min(nch, NZ / 8 > 0 ? NZ / 8 : 1));
-    fa.zchunk = (int)cdiv(NZ, nch);
-    nch = (int)cdiv(NZ, fa.zchunk);
     with_small(NX, [&](auto cn) {
       constexpr int N = decltype(cn)::value;
-      launch(k_row_fused<T, N>, dim3(MY, nch), dim3(FusedCfg<N>::template threads<T>()), FusedCfg<N>::template smem<T>(), st, fa,
-             a, tw);
+      const int threads = FusedCfg<N>::template threads<T>();
+      const size_t smem = FusedCfg<N>::template smem<T>();
+      if (fused_chunks == 0) fused_chunks = fused_chunk_count((const void*)k_row_fused<T, N>, threads, smem);
+      fa.zchunk = (int)cdiv(NZ, fused_chunks);
+      launch(k_row_fused<T, N>, dim3(MY, (unsigned)cdiv(NZ, fa.zchunk)), dim3(threads), smem, st, fa, a, tw);
     });
+  }
+  // z chunks per padded row of the fused kernel: a CTA walks its chunk with
+  // a sliding window, so chunks only add prologues (about half a level of
+  // work each), while the last wave of CTAs leaves SMs idle.  Minimise
+  // waves x (levels per chunk + 1/2) over 1..NZ/8 chunks, the waves counted
+  // with the kernel's resident CTAs per SM.
+  int fused_chunks = 0;
+  int fused_chunk_count(const void* kernel, int threads, size_t smem) {
+    if (smem > 48 * 1024) set_smem_limit(kernel, smem);
+    int per_sm = 0;
+    LES_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    const double resident = (double)std::max(1, per_sm) * nsm;
+    int best = 1;
+    double best_cost = 0.0;
+    for (int c = 1; c <= std::max(1, NZ / 8); c++) {
+      const int zc = (int)cdiv(NZ, c), n = (int)cdiv(NZ, zc);
+      const double cost = std::ceil((double)MY * n / resident) * (zc + 0.5);
+      if (c == 1 || cost < best_cost) { best = c; best_cost = cost; }
+    }
+    return best;
   }
   void unfused_middle(const StageArgs& a) {
     Ptr8 msrc{};
