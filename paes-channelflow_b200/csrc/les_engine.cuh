@@ -491,8 +491,9 @@ struct Engine : EngineBase {
       for (int i = 0; i < 8; i++) X.p[i] = fused ? xout[i].p : mixed[i].p;  // Xu1..Xe2
       Ptr8 rn{};
       rn.p[0] = run.p; rn.p[1] = rvn.p; rn.p[2] = rwn.p; rn.p[3] = rem.p;
-      size_t smem = 2 * C::buf() + (size_t)C::TC * N * sizeof(cx<T>) + (size_t)(3 * N / 2) * sizeof(cx<T>);
-      launch(k_y_forward<T, N>, dim3(cdiv(KX, C::TC), NZ, 4), dim3(2 * C::THREADS), smem, st, X, rn, KX, NZ, (T)ky0,
+      // clusters of two CTAs (X1, X2) per column group
+      size_t smem = C::buf() + (size_t)(3 * N / 2) * sizeof(cx<T>);
+      launch(k_y_forward<T, N>, dim3(2 * cdiv(KX, C::TC), NZ, 4), dim3(C::THREADS), smem, st, X, rn, KX, NZ, (T)ky0,
              (T)(1.0 / ((double)MX * MY)), tw);
     });
     if (learned_on()) learned_post(a);

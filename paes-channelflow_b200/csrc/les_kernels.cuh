@@ -26,6 +26,8 @@
 //   k_press                     comprhs + press (tridv) per (kx, ky), FP64
 //   k_update                    comp2 in spectral space, FP64
 #pragma once
+#include <cooperative_groups.h>
+
 #include "fft_core.cuh"
 
 namespace les {
@@ -760,45 +762,57 @@ k_x_forward(Ptr11 in, Ptr8 out, int MY, int NZ, T kx0, const cx<T>* __restrict__
 //   R^(ky) = (FFT_M(X1) - i ky FFT_M(X2)) / (MX*MY) at the kept ky,
 // rw's plane mean removed (comp1.f90:172).  R^ of u, v, w is written to
 // rnew[f]; for e, re = IFFT_N(R^) (x-spectral) is written to rnew[3].
+// A cluster of two CTAs per column group (blockIdx.x = 2 group + rank):
+// rank 0 transforms X1, rank 1 X2, each into its own shared memory; after a
+// cluster barrier each rank combines half of the kept ky rows, reading the
+// other rank's transform through distributed shared memory (for e, rank 0
+// combines all rows in place and runs the inverse N-point transform after a
+// second cluster barrier).  Half the shared memory and threads of a CTA that
+// held both transforms: FP64 2.6% faster, FP32 unchanged.
 template <class T, int NS>
-__global__ void __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS * 2)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS)
 k_y_forward(Ptr8 X, Ptr8 rnew, int KX, int NZ, T ky0, T scale, const cx<T>* __restrict__ tw) {
   constexpr int M = 3 * NS / 2;
   using C = ColCfg<M, T>;
-  constexpr int TC2 = 2 * C::TC;
+  constexpr int TC = C::TC;
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
-  cx<T>* sm3 = sm + TC2 * M;
+  cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+  const int rank = (int)cluster.block_rank();
   const int f = blockIdx.z, z = blockIdx.y + 1;
   if (f >= 2 && z == NZ) return;
-  const int kx0 = blockIdx.x * C::TC;
-  const cx<T>* X1 = (const cx<T>*)X.p[2 * f] + (size_t)(z - 1) * M * KX;
-  const cx<T>* X2 = (const cx<T>*)X.p[2 * f + 1] + (size_t)(z - 1) * M * KX;
+  const int kx0 = (blockIdx.x >> 1) * TC;
+  const cx<T>* Xs = (const cx<T>*)X.p[2 * f + rank] + (size_t)(z - 1) * M * KX;
   // the twiddles of the M-point transform staged in shared memory (measured
   // faster here than reading them through L1)
-  const cx<T>* tws = stage_twiddles<M>(sm3 + C::TC * NS, tw);
-  fft_core_tab<M, -1, true, false, true>(TC2, sm, tws, [&](int t, int n) {
-    int tt = t % C::TC, kx = kx0 + tt;
-    const cx<T>* src = (t < C::TC) ? X1 : X2;
-    return (kx < KX) ? src[(size_t)n * KX + kx] : zero_cx<T>();
+  const cx<T>* tws = stage_twiddles<M>(sm + (size_t)TC * M, tw);
+  fft_core_tab<M, -1, true, false, true>(TC, sm, tws, [&](int t, int n) {
+    int kx = kx0 + t;
+    return (kx < KX) ? Xs[(size_t)n * KX + kx] : zero_cx<T>();
   }, NoStore{});
+  cluster.sync();
+  const cx<T>* s1 = cluster.map_shared_rank(sm, 0);
+  const cx<T>* s2 = cluster.map_shared_rank(sm, 1);
   cx<T>* dst = (cx<T>*)rnew.p[f] + (size_t)(z - 1) * NS * KX;
-  for (int i = threadIdx.x; i < C::TC * NS; i += blockDim.x) {
-    int t = i % C::TC, ky = i / C::TC, kx = kx0 + t;
+  constexpr int ITEMS = TC * NS;
+  const int lo = (f == 3) ? 0 : rank * (ITEMS / 2);
+  const int hi = (f == 3) ? (rank == 0 ? ITEMS : 0) : lo + ITEMS / 2;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    int t = i % TC, ky = i / TC, kx = kx0 + t;
     int n = (ky < NS / 2) ? ky : ky + NS / 2;
     cx<T> v = zero_cx<T>();
     if (ky != NS / 2) {
-      cx<T> y1 = sm[n * TC2 + t], y2 = sm[n * TC2 + C::TC + t];
+      cx<T> y1 = s1[n * TC + t], y2 = s2[n * TC + t];
       T kk = ky0 * (T)signed_k(ky, NS);
-      v = mk(y1.x + kk * y2.y, y1.y - kk * y2.x) * scale;  // y1 - i ky y2
+      v = mk(y1.x + kk * y2.y, y1.y - kk * y2.x) * scale;
       if (f == 2 && kx == 0 && ky == 0) v = zero_cx<T>();
     }
     if (f < 3) { if (kx < KX) dst[(size_t)ky * KX + kx] = v; }
-    else sm3[ky * C::TC + t] = v;
+    else sm[ky * TC + t] = v;
   }
-  if (f == 3) {
-    __syncthreads();
-    fft_core<NS, +1, true, true, false>(C::TC, sm3, tw, NoLoad{}, [&](int t, int n, cx<T> v) {
+  cluster.sync();
+  if (f == 3 && rank == 0) {
+    fft_core<NS, +1, true, true, false>(TC, sm, tw, NoLoad{}, [&](int t, int n, cx<T> v) {
       int kx = kx0 + t;
       if (kx < KX) dst[(size_t)n * KX + kx] = v;
     });
