@@ -213,6 +213,11 @@ struct Engine : EngineBase {
   // staging for transfers (small-grid physical)
   DevBuf<T> phys[4];
   DevBuf<unsigned char> stage_buf;
+  // L2 prefetch of the y-column tiles by the TMA (les_tma.cuh): tensor maps
+  // of k_y_inverse's spectral inputs and k_y_forward's mixed inputs, and the
+  // prefetch distance in blocks (one resident wave; 0 = no prefetch)
+  ColMaps yinv_maps{}, yfwd_maps{};
+  unsigned yinv_pdist = 0, yfwd_pdist = 0;
   // learned closure (imodel = LES_SGS_LEARNED with a network attached)
   const MlpDev* mlp = nullptr;
   double re_tau = 0.0;
@@ -275,6 +280,32 @@ struct Engine : EngineBase {
     wp.alloc(1); err.alloc(1); amax.alloc(4);
     for (auto& b : phys) b.alloc(ps * (NZ + 2));
     stage_buf.alloc(ps * NZ * 8);
+    with_small(NY, [&](auto cn) { y_prefetch_setup<decltype(cn)::value>(); });
+  }
+  // Tensor maps and distances of the y-column prefetches.  The distance is
+  // one resident wave of the kernel (resident blocks per SM x SMs, even so
+  // that a k_y_forward block prefetches for a block of its own cluster rank
+  // and a k_y_inverse field block for a field block); one wave ahead measured
+  // faster than two or more.  Without the driver's tensor-map encoder or
+  // with a geometry the TMA cannot box, the distance stays 0.
+  template <int N> void y_prefetch_setup() {
+    using CM = ColCfg<3 * N / 2, T>;
+    auto wave = [&](const void* k, size_t smem) -> unsigned {
+      if (smem > 48 * 1024) set_smem_limit(k, smem);
+      int nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, CM::THREADS, smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+      }
+      return (unsigned)(nb * nsm) & ~1u;
+    };
+    void* src[4] = {uh.p, vh.p, wh.p, Xe.p};
+    if (make_col_maps<T, N, CM::TC>(yinv_maps, src, 4, KX, NZ))
+      yinv_pdist = wave((const void*)k_y_inverse<T, N>, CM::buf());
+    void* X[8];
+    for (int i = 0; i < 8; i++) X[i] = fused ? xout[i].p : mixed[i].p;
+    if (make_col_maps<T, 3 * N / 2, CM::TC>(yfwd_maps, X, 8, KX, NZ))
+      yfwd_pdist = wave((const void*)k_y_forward<T, N>, CM::buf() + (size_t)(3 * N / 2) * sizeof(cx<T>));
   }
   ~Engine() override {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -477,7 +508,7 @@ struct Engine : EngineBase {
       src.p[0] = uh.p; src.p[1] = vh.p; src.p[2] = wh.p; src.p[3] = Xe.p;
       for (int i = 0; i < 8; i++) dst.p[i] = mixed[i].p;
       launch(k_y_inverse<T, N>, dim3(2 * cdiv(KX, CM::TC), NZ, 4), dim3(CM::THREADS), CM::buf(), st, src, dst,
-             KX, NZ, (T)ky0, tw);
+             KX, NZ, (T)ky0, tw, yinv_maps, yinv_pdist);
     });
     if (fused) {
       fused_middle(a);
@@ -494,7 +525,7 @@ struct Engine : EngineBase {
       // clusters of two CTAs (X1, X2) per column group
       size_t smem = C::buf() + (size_t)(3 * N / 2) * sizeof(cx<T>);
       launch(k_y_forward<T, N>, dim3(2 * cdiv(KX, C::TC), NZ, 4), dim3(C::THREADS), smem, st, X, rn, KX, NZ, (T)ky0,
-             (T)(1.0 / ((double)MX * MY)), tw);
+             (T)(1.0 / ((double)MX * MY)), tw, yfwd_maps, yfwd_pdist);
     });
     if (learned_on()) learned_post(a);
   }

@@ -29,6 +29,7 @@
 #include <cooperative_groups.h>
 
 #include "fft_core.cuh"
+#include "les_tma.cuh"
 
 namespace les {
 
@@ -282,11 +283,21 @@ struct Ptr12 { void* p[12]; };
 // the columns from L2: half the block of a paired form, so that two blocks
 // share an SM and one's loads overlap the other's transform and stores
 // (measured 22% faster in FP32 than TC paired transforms per block).
+// Thread 0 of a field block first has the TMA prefetch into L2 the columns
+// of the field block `pdist` blocks ahead (les_tma.cuh; maps: tensor maps of
+// src[0..3] as [NZ*NS][KX] rows; pdist 0 prefetches nothing).
 template <class T, int NS>
 __global__ void __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS)
-k_y_inverse(Ptr8 src, Ptr8 dst, int KX, int NZ, T ky0, const cx<T>* __restrict__ tw) {
+k_y_inverse(Ptr8 src, Ptr8 dst, int KX, int NZ, T ky0, const cx<T>* __restrict__ tw,
+            const __grid_constant__ ColMaps maps, unsigned pdist) {
   constexpr int M = 3 * NS / 2;
   using C = ColCfg<M, T>;
+  if ((blockIdx.x & 1) == 0)
+    prefetch_tile_ahead<T, NS, C::TC>(maps, pdist, [&](unsigned bx, unsigned by, unsigned bz, int& q, int& cg,
+                                                       int& row0) {
+      q = (int)bz; cg = (int)(bx >> 1); row0 = (int)by * NS;
+      return !(bz >= 2 && (int)by + 1 == NZ);
+    });
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
   const int f = blockIdx.z, h = blockIdx.x & 1, z = blockIdx.y + 1;
@@ -768,13 +779,21 @@ k_x_forward(Ptr11 in, Ptr8 out, int MY, int NZ, T kx0, const cx<T>* __restrict__
 // other rank's transform through distributed shared memory (for e, rank 0
 // combines all rows in place and runs the inverse N-point transform after a
 // second cluster barrier).  Half the shared memory and threads of a CTA that
-// held both transforms: FP64 2.6% faster, FP32 unchanged.
+// held both transforms: FP64 2.6% faster, FP32 unchanged.  Thread 0 first
+// has the TMA prefetch into L2 the columns of the block `pdist` blocks
+// ahead (les_tma.cuh; maps: tensor maps of X[0..7] as [NZ*M][KX] rows;
+// pdist 0 prefetches nothing).
 template <class T, int NS>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(ColCfg<3 * NS / 2, T>::THREADS)
-k_y_forward(Ptr8 X, Ptr8 rnew, int KX, int NZ, T ky0, T scale, const cx<T>* __restrict__ tw) {
+k_y_forward(Ptr8 X, Ptr8 rnew, int KX, int NZ, T ky0, T scale, const cx<T>* __restrict__ tw,
+            const __grid_constant__ ColMaps maps, unsigned pdist) {
   constexpr int M = 3 * NS / 2;
   using C = ColCfg<M, T>;
   constexpr int TC = C::TC;
+  prefetch_tile_ahead<T, M, TC>(maps, pdist, [&](unsigned bx, unsigned by, unsigned bz, int& q, int& cg, int& row0) {
+    q = 2 * (int)bz + (int)(bx & 1); cg = (int)(bx >> 1); row0 = (int)by * M;
+    return !(bz >= 2 && (int)by + 1 == NZ);
+  });
   extern __shared__ __align__(16) unsigned char smraw[];
   cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
   cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
