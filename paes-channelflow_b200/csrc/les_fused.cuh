@@ -398,6 +398,20 @@ k_row_fused(FusedArgs f, StageArgs a, const cx<T>* __restrict__ tw) {
       }
     }
     __syncthreads();
+    // L2 prefetch (one thread, nothing waits on it) of the rows the next
+    // level's phase I reads from DRAM: U, V, W, E at z+2 and VY, UY, WY, EY at
+    // z+1 (U, V, W, E at z+1 were this level's window rows and are in L2)
+    if (threadIdx.x == 0 && z + 1 <= z1) {
+      constexpr unsigned RB = KX * sizeof(cx<T>);
+      if (z + 2 <= NZ) { tma::prefetch_l2(mixrow(0, z + 2), RB); tma::prefetch_l2(mixrow(2, z + 2), RB); }
+      if (z + 2 <= NZ - 1) { tma::prefetch_l2(mixrow(4, z + 2), RB); tma::prefetch_l2(mixrow(6, z + 2), RB); }
+      tma::prefetch_l2(mixrow(3, z + 1), RB);
+      if (!learned) tma::prefetch_l2(mixrow(1, z + 1), RB);
+      if (z + 1 <= NZ - 1) {
+        if (!learned) tma::prefetch_l2(mixrow(5, z + 1), RB);
+        tma::prefetch_l2(mixrow(7, min(z + 1, NZ - 2)), RB);
+      }
+    }
     // ---- phase II: fluxes (k_flux) ----
     // the forward transforms of F+iPe and H reuse the z-1 window slots,
     // whose rows are dead once each point has read them

@@ -18,6 +18,9 @@
 // The arrays are described to the TMA as 2-D tensors of real elements:
 // dim 0 the 2KX reals of one row, dim 1 all rows of all levels.  A tile is
 // NB boxes of 2TC x BR elements, BR = rows / NB <= 256.
+//
+// tma::prefetch_l2 is the untiled form (one contiguous range), used by
+// k_row_fused for the rows its next sliding-window level reads.
 #pragma once
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -33,6 +36,12 @@ __device__ __forceinline__ void prefetch_2d(const CUtensorMap* map, int x, int y
   asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
                    reinterpret_cast<uint64_t>(map)),
                "r"(x), "r"(y)
+               : "memory");
+}
+// Prefetch into L2 `bytes` contiguous bytes at `p` (16-byte aligned, a
+// multiple of 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(p)), "r"(bytes)
                : "memory");
 }
 }  // namespace tma
