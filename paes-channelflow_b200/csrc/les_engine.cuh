@@ -388,21 +388,33 @@ struct Engine : EngineBase {
     }
     LES_CUDA(cudaStreamSynchronize(st));
   }
-  static void host_plane_means(const void* h, int rb, int NZ_, size_t P, std::vector<double>& out) {
-    out.assign(NZ_, 0.0);
-    for (int z = 0; z < NZ_; z++) {
-      double s = 0;
-      if (rb == 8) { const double* a = (const double*)h + (size_t)z * P; for (size_t i = 0; i < P; i++) s += a[i]; }
-      else { const float* a = (const float*)h + (size_t)z * P; for (size_t i = 0; i < P; i++) s += a[i]; }
-      out[z] = s / (double)P;
-    }
+  // FP64 plane means of the uploaded field, summed on the device in a fixed
+  // order (k_plane_sums, one block per level) over the device copy of the
+  // host values in their own width: phys[0] when the host reals are T, the
+  // staging buffer h2d copied them to otherwise.
+  void uploaded_plane_means(int rb, std::vector<double>& out) {
+    LES_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)NZ * 16 * sizeof(double), st));
+    if (rb == (int)sizeof(T))
+      launch(k_plane_sums<T>, dim3(1, NZ), dim3(1024), 0, st, (const T*)phys[0].p, (const T*)nullptr,
+             (const T*)nullptr, (const T*)nullptr, ps, acc.p);
+    else if (rb == 8)
+      launch(k_plane_sums<double>, dim3(1, NZ), dim3(1024), 0, st, (const double*)stage_buf.p,
+             (const double*)nullptr, (const double*)nullptr, (const double*)nullptr, ps, acc.p);
+    else
+      launch(k_plane_sums<float>, dim3(1, NZ), dim3(1024), 0, st, (const float*)stage_buf.p, (const float*)nullptr,
+             (const float*)nullptr, (const float*)nullptr, ps, acc.p);
+    std::vector<double> s((size_t)NZ * 8);
+    LES_CUDA(cudaMemcpyAsync(s.data(), acc.p, s.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    out.resize(NZ);
+    for (int z = 0; z < NZ; z++) out[z] = s[(size_t)z * 8] / (double)ps;
   }
   void upload_spectral(const void* h, int rb, cx<T>* dst, double* shadow, bool zero_top) {
     h2d(h, phys[0].p, ps * NZ, rb);
+    std::vector<double> m;
+    if (shadow) uploaded_plane_means(rb, m);  // before to_spectral: the staging buffer is still the host data
     to_spectral(phys[0].p, dst, NZ);
     if (shadow) {
-      std::vector<double> m;
-      host_plane_means(h, rb, NZ, ps, m);
       LES_CUDA(cudaMemcpyAsync(shadow, m.data(), NZ * sizeof(double), cudaMemcpyHostToDevice, st));
       launch(k_set_mean<T>, dim3(cdiv(NZ, 128)), dim3(128), 0, st, dst, (const double*)shadow, nm, NZ);
       LES_CUDA(cudaStreamSynchronize(st));
